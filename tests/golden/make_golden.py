@@ -1,0 +1,51 @@
+"""Extract the reference's own known answers for this path into lam_pins.npz.
+
+Run once in a checkout that has the reference tree (the path is given on the
+command line; default /root/reference).  The output is committed so that the
+tests need no access to the reference at run time.
+
+What is taken, all from polyorder-master.zip:example/AB/LAM/ (the upstream
+PolyOrder snapshot bundled in the reference):
+
+* 1D/field_in_64.mat, 2D/field_in_32x32.mat: the input fields wA, wB used by
+  those example runs (Grid gridInitType = File).
+* {1D,2D}/cell_opt_{rqm4,rqm4_anderson,os2,os2_anderson}.mat: the (a, F)
+  pairs written by scft::save_cell (src/scft.cc:589-609) during the Brent
+  cell optimisation.  Every entry is a converged SCFT free energy H at cell
+  size a (1D: thresh_residual 1e-8; 2D: 1e-6), with Ms = [51, 51],
+  chiN = 30, f = 0.5, incompressible, Simpson contour integration,
+  lam = [0.05, 0.05, 5.0], n_Anderson_mixing = 5 (the param.ini files).
+"""
+import io
+import os
+import sys
+import zipfile
+
+import numpy as np
+import scipy.io
+
+
+def main(ref_root="/root/reference"):
+    z = zipfile.ZipFile(os.path.join(ref_root, "polyorder-master.zip"))
+    base = "polyorder-master/example/AB/LAM/"
+    out = {}
+    f1 = scipy.io.loadmat(io.BytesIO(z.read(base + "1D/field_in_64.mat")))
+    out["lam1d_wA"] = np.asarray(f1["wA"], dtype=np.float64).reshape(64, 1, 1)
+    out["lam1d_wB"] = np.asarray(f1["wB"], dtype=np.float64).reshape(64, 1, 1)
+    f2 = scipy.io.loadmat(io.BytesIO(z.read(base + "2D/field_in_32x32.mat")))
+    out["lam2d_wA"] = np.asarray(f2["wA"], dtype=np.float64).reshape(32, 32, 1)
+    out["lam2d_wB"] = np.asarray(f2["wB"], dtype=np.float64).reshape(32, 32, 1)
+    for dim in ("1D", "2D"):
+        for tag in ("rqm4", "rqm4_anderson", "os2", "os2_anderson"):
+            name = base + "%s/cell_opt_%s.mat" % (dim, tag)
+            d = scipy.io.loadmat(io.BytesIO(z.read(name)))
+            key = "%s_%s" % (dim.lower(), tag)
+            out[key + "_a"] = np.asarray(d["a"], dtype=np.float64).ravel()
+            out[key + "_F"] = np.asarray(d["F"], dtype=np.float64).ravel()
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lam_pins.npz")
+    np.savez_compressed(dst, **out)
+    print("wrote", dst, sorted(out))
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -1,0 +1,169 @@
+"""Pins for the CPU oracle (oracle/scft_oracle.c) -- no GPU needed.
+
+The oracle is trusted only after these pass:
+* its FFT against numpy.fft (pocketfft);
+* its RQM4 / OS2 propagators against the independent NumPy restatement;
+* analytic identities the reference's own tests use (uniform fields,
+  quadrature KAT of tests/test_quadrature4.cc, k-table identity of
+  tests/test_unitcell.cc);
+* the reference's published converged free energies (LAM examples bundled in
+  polyorder-master.zip, extracted by tests/golden/make_golden.py).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import numpy_ref as nr
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _build():
+    oracle.build()
+
+
+@pytest.mark.parametrize("shape", [(8, 1, 1), (12, 1, 1), (64, 1, 1), (6, 10, 1), (32, 32, 1),
+                                   (48, 48, 1), (4, 6, 9), (7, 5, 3), (16, 12, 18)])
+def test_fft_matches_numpy(shape):
+    rng = np.random.default_rng(11)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    f = oracle.fft3(a, -1)
+    b = oracle.fft3(a, +1)
+    np.testing.assert_allclose(f, np.fft.fftn(a), rtol=0, atol=1e-13 * np.abs(f).max())
+    np.testing.assert_allclose(b, np.fft.ifftn(a) * a.size, rtol=0, atol=1e-13 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("shape,dim,L", [((16, 1, 1), 1, (3.0,)), ((12, 16, 1), 2, (3.0, 4.0)),
+                                         ((8, 6, 12), 3, (3.1, 3.2, 3.3))])
+def test_propagators_match_numpy(shape, dim, L):
+    rng = np.random.default_rng(1)
+    w = rng.standard_normal(shape)
+    k2 = oracle.k2_orthogonal(dim, L, shape)
+    assert np.array_equal(k2, nr.k2_orthogonal(dim, L, shape))
+    qs = np.zeros((21,) + shape)
+    qs[0] = 1 + 0.1 * rng.standard_normal(shape)
+    q1 = oracle.Updater("RQM4", k2, shape, 0.01).solve(w, qs.copy())
+    q2 = nr.rqm4_solve(w, qs.copy(), k2, 0.01)
+    np.testing.assert_allclose(q1, q2, rtol=1e-13, atol=0)
+    lap = np.exp(0.01 * k2)
+    q3 = oracle.Updater("OS2", lap, shape, 0.01).solve(w, qs.copy())
+    q4 = nr.os2_solve(w, qs.copy(), lap, 0.01)
+    np.testing.assert_allclose(q3, q4, rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("mde", ["RQM4", "OS2"])
+def test_uniform_field_is_exact(mde):
+    """With w constant only k=0 survives: q(s) = exp(-w s), so
+    Q = exp(-wA fA - wB fB), phiA = fA, phiB = fB (tests/test_density.cc:66-78)."""
+    shape = (8, 6, 4)
+    m = oracle.ModelAB(3, shape, (3.0, 3.5, 4.0), (31, 71), 20.0, mde=mde).init_fields(
+        np.full(shape, 0.1), np.full(shape, 0.3))
+    m.update()
+    fA, fB = 0.3, 0.7
+    assert abs(m.Q() - np.exp(-0.1 * fA - 0.3 * fB)) < 5e-14
+    np.testing.assert_allclose(m.get("phiA"), fA, rtol=0, atol=5e-14)
+    np.testing.assert_allclose(m.get("phiB"), fB, rtol=0, atol=5e-14)
+
+
+@pytest.mark.parametrize("rule,n,order_tol", [
+    (oracle.SIMPSON, 36, 1e-9), (oracle.QUAD4_CLOSED, 36, 1e-8), (oracle.QUAD4_CLOSED, 45, 1e-8),
+    (oracle.QUAD4_OPEN, 36, 1e-7), (oracle.QUAD4_SEMIOPEN_LEFT, 36, 1e-7),
+    (oracle.QUAD4_SEMIOPEN_RIGHT, 36, 1e-7), (oracle.TRAPEZOID, 36, 1e-4)])
+def test_quadrature_kat(rule, n, order_tol):
+    """q = 1, qc[s] = exp(s ds): phi = exp(n ds) - 1 up to the rule's
+    truncation error (tests/test_quadrature4.cc:58-100)."""
+    ds = 0.01
+    shape = (4, 1, 1)
+    q = np.ones((n + 1,) + shape)
+    qc = np.stack([np.full(shape, np.exp(s * ds)) for s in range(n + 1)])
+    phi = oracle.density(rule, q, qc, ds, 1.0)
+    exact = np.exp(n * ds) - 1.0
+    assert np.abs(phi - exact).max() < order_tol
+
+
+def test_quadrature_preconditions():
+    with pytest.raises(ValueError):
+        oracle.contour_weights(oracle.SIMPSON, 35)     # odd n (Simpson.cc:18-21)
+    with pytest.raises(ValueError):
+        oracle.contour_weights(oracle.SIMPSON, 2)      # n < 4 (Simpson.cc:22-25)
+    with pytest.raises(ValueError):
+        oracle.contour_weights(oracle.QUAD4_CLOSED, 6)  # n < 7 (Quadrature4.cc:22-25)
+
+
+def test_weights_match_numpy():
+    np.testing.assert_array_equal(oracle.contour_weights(oracle.SIMPSON, 30), nr.simpson_weights(30))
+    np.testing.assert_allclose(oracle.contour_weights(oracle.QUAD4_CLOSED, 45),
+                               nr.quad4_closed_weights(45), rtol=1e-15)
+
+
+@pytest.mark.parametrize("dim,system,cell,shape", [
+    (1, oracle.LAMELLAR, (3.3,), (16, 1, 1)),
+    (2, oracle.RECTANGULAR, (3.0, 4.5), (12, 10, 1)),
+    (3, oracle.ORTHORHOMBIC, (3.8, 4.0, 4.2), (8, 6, 10))])
+def test_klaplacian_matches_orthogonal(dim, system, cell, shape):
+    """calc_kLaplacian == exp(ds * calc_k2_orthogonal) on orthogonal cells
+    within 1e-10 (tests/test_unitcell.cc:40-70)."""
+    c = list(cell) + [0.0] * (3 - len(cell))
+    g, l = oracle.unit_cell(dim, system, c[0], c[1], c[2])
+    ds = 0.01
+    a = oracle.k_laplacian(g, shape, ds)
+    b = np.exp(ds * oracle.k2_orthogonal(dim, l, shape))
+    assert np.abs(a - b).max() < 1e-10
+
+
+def test_solve_small_matches_numpy():
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 5, 20):
+        A = rng.standard_normal((n, n)) + n * np.eye(n)
+        v = rng.standard_normal(n)
+        np.testing.assert_allclose(oracle.solve_small(A, v), np.linalg.solve(A, v), rtol=1e-12, atol=1e-12)
+
+
+def test_natural_spline_matches_scipy():
+    from scipy.interpolate import CubicSpline
+    rng = np.random.default_rng(5)
+    m, M = 9, 7
+    S = np.sort(np.concatenate([[0.0, 1.0], rng.uniform(0.05, 0.95, m - 2)]))
+    f = rng.standard_normal((m, M))
+    ref = np.stack([CubicSpline(S, f[:, i], bc_type="natural")(np.arange(m) / (m - 1)) for i in range(M)], 1)
+    g = f.copy()
+    oracle.string_redistribute(g, S, f[0], f[-1])
+    ref[0], ref[-1] = f[0], f[-1]
+    np.testing.assert_allclose(g, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_arclength():
+    rng = np.random.default_rng(6)
+    wa = rng.standard_normal((5, 3, 4, 1))
+    S = oracle.string_arclength(wa)
+    d = np.sqrt(((wa[1:] - wa[:-1]) ** 2).reshape(4, -1).mean(1))
+    ref = np.concatenate([[0.0], np.cumsum(d)])
+    np.testing.assert_allclose(S, ref / ref[-1], rtol=1e-14)
+
+
+def _converge(m, thresh, max_iter=20000):
+    r = None
+    for it in range(1, max_iter + 1):
+        m.update()
+        if it % 10 == 0 and it > 10:      # record_interval 10, min_iter 10 (param.ini)
+            r = m.residual()
+            if r < thresh:
+                break
+    return it, r
+
+
+@pytest.mark.parametrize("mde,scft,tag", [("RQM4", "EM", "1d_rqm4"), ("RQM4", "Anderson", "1d_rqm4_anderson"),
+                                          ("OS2", "EM", "1d_os2"), ("OS2", "Anderson", "1d_os2_anderson")])
+def test_published_free_energy_1d(golden, mde, scft, tag):
+    """Converged H on the reference's 1D LAM input (Lx=64, Ms=[51,51], chiN=30)
+    matches the F(a) table the reference wrote, at the residual threshold the
+    reference used (1e-8)."""
+    a_tab = golden[tag + "_a"]
+    F_tab = golden[tag + "_F"]
+    wA, wB = golden["lam1d_wA"], golden["lam1d_wB"]
+    for i in (0, 1, 4, len(a_tab) - 1):
+        m = oracle.ModelAB(1, (64, 1, 1), (a_tab[i],), (51, 51), 30.0, lam=(0.05, 0.05, 5.0),
+                           mde=mde, scft=scft, n_anderson=5).init_fields(wA, wB)
+        it, r = _converge(m, 1e-8)
+        assert r < 1e-8, (a_tab[i], it, r)
+        H = m.H()[0]
+        assert abs(H - F_tab[i]) < 3e-8, (a_tab[i], H, F_tab[i])
