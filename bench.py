@@ -1,0 +1,290 @@
+"""Benchmark of the periodic pseudospectral SCFT hot path on B200.
+
+Workload (one GPU): the 3D configuration -- AB diblock melt on a 64^3
+periodic cubic cell of 4.2 Rg, fA 0.35, chiN 25, Ns 200 (Ms [71, 131]),
+RQM4 propagators, Simpson contour integration, Anderson mixing with history
+20, FP64, seeded gyroid-plus-noise fields.  A step is one SCFT iteration
+(Model_AB::update: four propagators over 2 Ns contour steps, Q, densities,
+Anderson update).  Metric: gridpoint x contour-steps per second, 2 Ns M per
+step.  Inputs (the 0.8 GB propagator histories) exceed the 126 MB L2, so no
+explicit flush is done between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica (a single solve
+does not shard); value = total gridpoint-steps of all ranks / max time.
+--impl reference times the CPU restatement of the reference algorithm on the
+host cores (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "gridpt_contour_steps_per_s"
+UNIT = "gridpt*contour-steps/s"
+BYTES_PER_GRIDPT_STEP = 24.0       # read q_s, read w, write q_{s+1}
+WORKLOAD = "C2 Model_AB 3D 64^3 RQM4 Anderson(20) Ns=200 FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def config():
+    from polystring_b200 import workloads
+    return workloads.config("C2")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_gridpt_step():
+    """DRAM bytes per gridpoint-step of the propagator line passes from the
+    committed ncu summary (None until one exists)."""
+    path = os.path.join(ROOT, "profiles", "propagator_line_passes_64cube.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_gridpt_step:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(cfg, seconds, threads):
+    """Time the CPU oracle (the restatement of the reference's step sequence)
+    on a bounded sample: whole SCFT iterations of the same workload when one
+    fits in the time budget, else contour steps of the forward propagator."""
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
+    shape = cfg["shape"]
+    M = int(np.prod(shape))
+    L = cfg["cell"][1][0]
+    sA, sB = cfg["Ms"]
+    Ns = sA + sB - 2
+    k2 = oracle.k2_orthogonal(3, (L, L, L), shape)
+    ds = 1.0 / Ns
+    u = oracle.Updater("RQM4", k2, shape, ds)
+    qs = np.ones((2,) + shape)
+    t0 = time.perf_counter()
+    u.solve(cfg["wA"], qs)
+    one = time.perf_counter() - t0
+    nsteps = max(1, int(seconds / max(one, 1e-6)))
+    qs = np.ones((nsteps + 1,) + shape)
+    t0 = time.perf_counter()
+    u.solve(cfg["wA"], qs)
+    dt = time.perf_counter() - t0
+    return {"value": nsteps * M / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d RQM4 contour steps of one 64^3 propagator (oracle/scft_oracle.c, own FFT, "
+                      "%d OpenMP threads), %.1f s" % (nsteps, threads, dt)}
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm's CPU restatement on all host threads (rank 0);
+    each step is a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    cfg = config()
+    import oracle
+    threads = oracle.max_threads()
+    per = max(1.0, min(20.0, 120.0 / max(1, args.steps)))
+    for _ in range(args.warmup):
+        cpu_baseline(cfg, 0.2, threads)
+    vals = []
+    b = None
+    for _ in range(args.steps):
+        b = cpu_baseline(cfg, per, threads)
+        vals.append(b["value"])
+    v = float(np.median(vals))
+    Ns = sum(cfg["Ms"]) - 2
+    M = int(np.prod(cfg["shape"]))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2 * Ns * M / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded gyroid + noise fields)",
+            "config": {"workload": WORKLOAD, "grid": list(cfg["shape"]), "Ns": Ns, "l2_flush": "inputs > L2"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": b["sample"] + "; median of %d samples" % args.steps},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import polystring_b200 as ps
+    cfg = config()
+    shape = cfg["shape"]
+    M = int(np.prod(shape))
+    Ns = sum(cfg["Ms"]) - 2
+    units_per_step = 2 * Ns * M
+    cell = ps.make_cell(3, cfg["cell"][0], cfg["cell"][1][0])
+    m = ps.ModelAB(3, shape, cell, cfg["Ms"], cfg["chiN"], lam=cfg["lam"], mde=cfg["mde"], scft=cfg["scft"],
+                   n_anderson=cfg["n_anderson"])
+    m.set_fields(cfg["wA"], cfg["wB"])
+    m.update(args.warmup)
+    m.synchronize()
+
+    # ---- device-resident timed region --------------------------------------
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        # CUDA events on the model's stream around the K replays and around
+        # every propagator sweep inside them
+        total_ms, prop_ms = m.update_timed(args.steps)
+    barrier()
+    torch.cuda.synchronize()
+    total_s = allmax(total_ms / 1e3)
+    value = world * units_per_step * args.steps / total_s
+    launches = m.launches_per_iteration() * args.steps
+    H = m.H()[0]
+    if not np.isfinite(H):
+        raise RuntimeError("non-finite H after the timed region")
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    wA_h = torch.from_numpy(np.ascontiguousarray(cfg["wA"])).pin_memory()
+    wB_h = torch.from_numpy(np.ascontiguousarray(cfg["wB"])).pin_memory()
+    outs = [torch.empty(shape, dtype=torch.float64).pin_memory() for _ in range(4)]
+    K = args.steps
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.set_fields(wA_h.numpy(), wB_h.numpy())               # H2D of the inputs
+    for _ in range(K):
+        m.update(1)
+        m.H()                                              # D2H scalars each step (record_interval 1)
+        m.residual_error()
+    for o, name in zip(outs, ("wA", "wB", "phiA", "phiB")):
+        o.numpy()[...] = m.get(name)                       # D2H of the result fields
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e = {"value": world * units_per_step * K / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 2 * M * 8 / K, "d2h_bytes_per_step": (4 * M * 8 + 5 * 8 * K) / K}
+
+    # ---- roofline of the dominant kernel family (propagator line passes) ---
+    peak, peak_kind = peaks()
+    prop_s = allmax(prop_ms / 1e3)
+    achieved = BYTES_PER_GRIDPT_STEP * units_per_step * args.steps / prop_s / 1e9
+    tr = traffic_per_gridpt_step()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": tr * units_per_step if tr else None, "peak_kind": peak_kind,
+            "kernel": "propagator sweep (line-pass kernels), %d launches per iteration" % m.launches_per_propagate(),
+            "propagator_share_of_step": prop_s / total_s}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        import oracle
+        cpu = cpu_baseline(cfg, args.cpu_seconds, oracle.max_threads())
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded gyroid + noise fields)",
+                "config": {"workload": WORKLOAD, "grid": list(shape), "Ns": Ns, "Ms": list(cfg["Ms"]),
+                           "l2_flush": "inputs > L2 (0.8 GB histories)", "parallelism": "replicas" if world > 1 else "single"},
+                "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clk.summary(), "H_after": H}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

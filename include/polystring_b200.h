@@ -1,0 +1,175 @@
+/*
+ * polystring_b200.h -- C ABI of the B200 (sm_100a) implementation of
+ * PolyOrder's periodic pseudospectral SCFT path.
+ *
+ * Plain C: opaque handles, pointers and sizes; no C++ or torch types.  Every
+ * entry point returns PS_OK (0) or a negative status and never lets a C++
+ * exception cross the boundary; ps_last_error() gives the message of the
+ * last failure on the calling thread.
+ *
+ * Arrays are FP64, row-major (x, y, z) with z fastest, M = Lx*Ly*Lz points;
+ * a propagator history is len consecutive slices of M (slice s at qs + s*M),
+ * as Propagator stores _qs(len, Lx, Ly, Lz) (src/Propagator.cc:12-18).
+ * 2D grids use Lz = 1, 1D grids Ly = Lz = 1.  Supported axis lengths: 1, 2,
+ * 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256.
+ *
+ * Each context owns its device memory and one CUDA stream; a context is safe
+ * to use from one host thread at a time.  "_device" entry points take device
+ * pointers and a cudaStream_t passed as void* (NULL: the context's stream)
+ * and return without synchronising; the others take host pointers and
+ * return after the result is in host memory.
+ *
+ * Paths in the citations are relative to the reference project root.
+ */
+#ifndef POLYSTRING_B200_H
+#define POLYSTRING_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define PS_OK 0
+#define PS_ERR_INVALID (-1)      /* bad argument or cell                     */
+#define PS_ERR_UNSUPPORTED (-2)  /* grid size / history length not supported */
+#define PS_ERR_CUDA (-3)         /* CUDA runtime failure                     */
+#define PS_ERR_QUADRATURE (-4)   /* contour rule precondition fails          */
+#define PS_ERR_STATE (-6)        /* call out of order (e.g. H before update) */
+
+/* ---- enumerations ---------------------------------------------------- */
+/* MDE schemes, Config::algo_mde_type (src/Config.cc:1099-1111) */
+#define PS_MDE_RQM4 0            /* "RQM4" / "OS4": src/RQM4.cc              */
+#define PS_MDE_OS2 1             /* "OS2" / "PseudoSpectral": src/PseudoSpectral.cc */
+/* SCFT field update, Config::algo_scft_type (src/Config.cc:1219-1235) */
+#define PS_SCFT_EM 0
+#define PS_SCFT_ANDERSON 1
+/* contour integration rules */
+#define PS_CONTOUR_TRAPEZOID 0         /* Density::_update, src/Density.cc:107-121 */
+#define PS_CONTOUR_SIMPSON 1           /* Simpson::solve, src/Simpson.cc:14-45     */
+#define PS_CONTOUR_QUAD4_CLOSED 2      /* src/Quadrature4.cc:17-53                 */
+#define PS_CONTOUR_QUAD4_OPEN 3        /* src/Quadrature4.cc:62-102                */
+#define PS_CONTOUR_QUAD4_SEMIOPEN_LEFT 4  /* src/Quadrature4.cc:111-155            */
+#define PS_CONTOUR_QUAD4_SEMIOPEN_RIGHT 5 /* src/Quadrature4.cc:164-197            */
+/* crystal systems, UnitCell::calc_shape_matrix{1,2,3} (src/UnitCell.cc:149-296) */
+#define PS_CELL_LAMELLAR 0
+#define PS_CELL_SQUARE 1
+#define PS_CELL_RECTANGULAR 2
+#define PS_CELL_HEXAGONAL2 3
+#define PS_CELL_OBLIQUE 4
+#define PS_CELL_CUBIC 5
+#define PS_CELL_TETRAGONAL 6
+#define PS_CELL_ORTHORHOMBIC 7
+#define PS_CELL_HEXAGONAL3 8
+#define PS_CELL_TRIGONAL 9
+#define PS_CELL_MONOCLINIC 10
+#define PS_CELL_TRICLINIC 11
+/* ps_model_ab_get / ps_model_ab_device_ptr: which array */
+#define PS_FIELD_WA 0
+#define PS_FIELD_WB 1
+#define PS_FIELD_PHIA 2
+#define PS_FIELD_PHIB 3
+#define PS_FIELD_YITA 4
+#define PS_FIELD_QA 5    /* sA slices */
+#define PS_FIELD_QB 6    /* sB slices */
+#define PS_FIELD_QAC 7   /* sA slices */
+#define PS_FIELD_QBC 8   /* sB slices */
+
+/* UnitCell parameters ([UnitCell] a, b, c, alpha, beta, gamma; angles in
+ * radians), replacing UnitCell(const Config&) (include/UnitCell.h:39-98). */
+typedef struct ps_unit_cell {
+    int dim;
+    int system;
+    double a, b, c;
+    double alpha, beta, gamma;
+} ps_unit_cell;
+
+typedef struct ps_updater ps_updater;
+typedef struct ps_model_ab ps_model_ab;
+
+const char* ps_version(void);
+const char* ps_last_error(void);
+
+/* ---- propagator updaters (the Updater interface, include/Updater.h:44-69) */
+
+/* RQM4(const UnitCell&, Lx, Ly, Lz, ds)            src/RQM4.cc:9-16
+ * PseudoSpectral(const UnitCell&, Lx, Ly, Lz, ds)  src/PseudoSpectral.cc:190-195
+ * scheme = PS_MDE_RQM4 or PS_MDE_OS2. */
+int ps_updater_create(int scheme, const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds,
+                      ps_updater** out);
+/* Updater::clone() (include/Updater.h:67) */
+int ps_updater_clone(const ps_updater* u, ps_updater** out);
+void ps_updater_destroy(ps_updater* u);
+/* Updater::solve(Propagator& q, const Grid& w) (include/Updater.h:55;
+ * src/RQM4.cc:41-93, src/PseudoSpectral.cc:226-261): qs[0] is the head on
+ * entry; slices 1..len-1 are overwritten. */
+int ps_updater_solve(ps_updater* u, const double* w, double* qs, int len);
+int ps_updater_solve_device(ps_updater* u, const double* w, double* qs, int len, void* stream);
+
+/* ---- density (Updater::solve(data, q, qc, cc), include/Updater.h:57-58) */
+/* phi = cc * ds * sum_s c_s q[s] qc[len-1-s] with the weights of `rule`.
+ * Returns PS_ERR_QUADRATURE when the rule's precondition fails (the
+ * reference prints to cerr and leaves phi unchanged, src/Simpson.cc:18-26). */
+int ps_density_solve(int rule, const double* q, const double* qc, int len, long long M, double ds, double cc,
+                     double* phi);
+int ps_density_solve_device(int rule, const double* q, const double* qc, int len, long long M, double ds,
+                            double cc, double* phi, void* stream);
+
+/* Grid::quadrature on a regular grid: the mean (src/Grid.cc:329-374); with
+ * a propagator slice this is Propagator::Q(s) (src/Propagator.cc:85-89). */
+int ps_grid_mean_device(const double* x, long long M, double* out_host, void* stream);
+
+/* ---- Model_AB: the whole SCFT iteration on the device ---------------- */
+/* Fields of the reference's config file that Model_AB reads. */
+typedef struct ps_model_ab_params {
+    int dim, Lx, Ly, Lz;       /* [Grid] dimension, Lx, Ly, Lz                  */
+    ps_unit_cell cell;         /* [UnitCell]                                    */
+    int sA, sB;                /* [Algorithm_MDE] Ms                            */
+    double chiN;               /* [Model] chiN                                  */
+    double lamA, lamB, lamYita;/* [Algorithm_SCFT] lam                          */
+    int mde;                   /* PS_MDE_*                                      */
+    int scft;                  /* PS_SCFT_*                                     */
+    int n_anderson;            /* [Algorithm_SCFT] n_Anderson_mixing (1..31)    */
+    int compressible;          /* [Model] is_compressible                       */
+    int contour;               /* 0 trapezoid, 1 Simpson (Simpson / Quad4_Closed
+                                  by parity of Ms, src/Model_AB.cc:713-735)     */
+} ps_model_ab_params;
+
+/* Model_AB::init (src/Model_AB.cc:85-134) for a periodic cell */
+int ps_model_ab_create(const ps_model_ab_params* p, ps_model_ab** out);
+void ps_model_ab_destroy(ps_model_ab* m);
+/* DATA_INIT fields (Model_AB::init_data_field, src/Model_AB.cc:672-675;
+ * resetInString, :52-83): sets wA, wB, zeroes yita, restarts Anderson. */
+int ps_model_ab_set_fields(ps_model_ab* m, const double* wA, const double* wB);
+int ps_model_ab_set_fields_device(ps_model_ab* m, const double* wA, const double* wB);
+/* n_iter x Model_AB::update (src/Model_AB.cc:136-261), the loop body of
+ * scft::relax (src/scft.cc:395-397).  Asynchronous on the context stream. */
+int ps_model_ab_update(ps_model_ab* m, int n_iter);
+/* ps_model_ab_update with CUDA events on the context stream around the
+ * whole run and around every propagator sweep; synchronises, then returns
+ * the device time of the run and the summed sweep time, in milliseconds. */
+int ps_model_ab_update_timed(ps_model_ab* m, int n_iter, double* total_ms, double* propagator_ms);
+/* n_iter x the four Propagator::update calls of Model_AB::update only
+ * (qA, qB, qBc, qAc; src/Model_AB.cc:187-193), no density or mixing. */
+int ps_model_ab_propagate(ps_model_ab* m, int n_iter);
+/* Model_AB::H / Hw / Hs (src/Model_AB.cc:263-300) */
+int ps_model_ab_H(ps_model_ab* m, double* H, double* Hw, double* Hs);
+/* Model_AB::residual_error (src/Model_AB.cc:307-371) */
+int ps_model_ab_residual(ps_model_ab* m, double* res);
+/* qB->Qt() of the last update (src/Model_AB.cc:195) */
+int ps_model_ab_Q(ps_model_ab* m, double* Q);
+/* copy one array (PS_FIELD_*) to host memory */
+int ps_model_ab_get(ps_model_ab* m, int which, double* out);
+/* device address of one array (PS_FIELD_*), owned by the context */
+int ps_model_ab_device_ptr(ps_model_ab* m, int which, double** out);
+int ps_model_ab_synchronize(ps_model_ab* m);
+/* kernel launches of one iteration / of one propagator sweep pair */
+int ps_model_ab_launches_per_iteration(ps_model_ab* m);
+int ps_model_ab_launches_per_propagate(ps_model_ab* m);
+/* CUDA stream of the context (cudaStream_t as void*) */
+void* ps_model_ab_stream(ps_model_ab* m);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLYSTRING_B200_H */

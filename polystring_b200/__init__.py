@@ -1,0 +1,199 @@
+"""polystring_b200 -- B200 (sm_100a, FP64) implementation of PolyOrder's
+periodic pseudospectral SCFT path behind the reference's Updater / Model
+interface.
+
+The compute path is libpolystring_b200.so (hand-written CUDA, C ABI in
+include/polystring_b200.h); this module is a thin Python mirror of the
+reference's classes over that ABI:
+
+    RQM4(cell, Lx, Ly, Lz, ds).solve(qs, w)        src/RQM4.cc:9-93
+    PseudoSpectral(cell, Lx, Ly, Lz, ds).solve(..)  src/PseudoSpectral.cc:190-261
+    density(rule, q, qc, ds, cc)                    src/Simpson.cc, src/Quadrature4.cc
+    ModelAB(...).update(), H(), residual_error()    src/Model_AB.cc:85-371
+
+Host numpy arrays go through the host entry points; torch CUDA tensors go
+through the "_device" entry points without copies.  There is no CPU
+fallback: without the built library every entry point raises ImportError.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import PSError, make_cell, FIELDS, RULES
+
+__all__ = ["RQM4", "PseudoSpectral", "ModelAB", "density", "grid_mean", "make_cell", "PSError", "lib"]
+
+
+def lib():
+    """The loaded CUDA library; raises ImportError when it is not built."""
+    return capi.load()
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _Updater:
+    scheme = None
+
+    def __init__(self, cell, Lx, Ly, Lz, ds):
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_updater_create(self.scheme, ctypes.byref(cell), Lx, Ly, Lz, ds, ctypes.byref(h)))
+        self._h = h
+        self.shape = (Lx, Ly, Lz)
+        self.M = Lx * Ly * Lz
+
+    def clone(self):
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_updater_clone(self._h, ctypes.byref(h)))
+        c = object.__new__(type(self))
+        c._h, c.shape, c.M = h, self.shape, self.M
+        return c
+
+    def solve(self, qs, w, stream=None):
+        """Updater::solve(Propagator& q, const Grid& w): qs (len, Lx, Ly, Lz),
+        qs[0] is the head; slices 1.. are overwritten in place."""
+        if _is_torch(qs):
+            assert qs.is_cuda and w.is_cuda and qs.is_contiguous() and w.is_contiguous()
+            capi.check(lib().ps_updater_solve_device(self._h, w.data_ptr(), qs.data_ptr(), qs.shape[0],
+                                                     stream if stream is not None else None))
+            return qs
+        assert qs.dtype == np.float64 and qs.flags.c_contiguous
+        w = _f64(w)
+        capi.check(lib().ps_updater_solve(self._h, capi.dptr(w), capi.dptr(qs), qs.shape[0]))
+        return qs
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().ps_updater_destroy(h)
+            self._h = None
+
+
+class RQM4(_Updater):
+    """4th-order Richardson-extrapolated operator splitting (src/RQM4.cc)."""
+    scheme = 0
+
+
+class PseudoSpectral(_Updater):
+    """2nd-order operator splitting, general-cell Laplacian (src/PseudoSpectral.cc)."""
+    scheme = 1
+
+
+def density(rule, q, qc, ds, cc):
+    """phi = cc ds sum_s c_s q[s] qc[n-s] (Simpson / Quad4 / trapezoid)."""
+    r = RULES[rule] if isinstance(rule, str) else int(rule)
+    q = _f64(q)
+    qc = _f64(qc)
+    M = int(np.prod(q.shape[1:]))
+    phi = np.zeros(q.shape[1:])
+    capi.check(lib().ps_density_solve(r, capi.dptr(q), capi.dptr(qc), q.shape[0], M, ds, cc, capi.dptr(phi)))
+    return phi
+
+
+def grid_mean(x_cuda):
+    """Grid::quadrature of a CUDA tensor (deterministic device reduction)."""
+    out = ctypes.c_double()
+    capi.check(lib().ps_grid_mean_device(x_cuda.data_ptr(), x_cuda.numel(), ctypes.byref(out), None))
+    return out.value
+
+
+class ModelAB:
+    """Model_AB on the device: one SCFT iteration is one replay of a captured
+    CUDA graph (propagators, Q, densities, field update)."""
+
+    def __init__(self, dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft="EM",
+                 n_anderson=5, compressible=False, contour="Simpson"):
+        Lx, Ly, Lz = shape
+        p = capi.ModelABParamsC()
+        p.dim, p.Lx, p.Ly, p.Lz = dim, Lx, Ly, Lz
+        p.cell = cell
+        p.sA, p.sB = Ms
+        p.chiN = chiN
+        p.lamA, p.lamB, p.lamYita = lam
+        p.mde = capi.MDE[mde.upper()]
+        p.scft = capi.SCFT[scft.upper()]
+        p.n_anderson = n_anderson
+        p.compressible = 1 if compressible else 0
+        p.contour = capi.CONTOUR[contour.upper()]
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_model_ab_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.shape = tuple(shape)
+        self.M = Lx * Ly * Lz
+        self.Ms = tuple(Ms)
+
+    def set_fields(self, wA, wB):
+        if _is_torch(wA):
+            capi.check(lib().ps_model_ab_set_fields_device(self._h, wA.data_ptr(), wB.data_ptr()))
+        else:
+            wA, wB = _f64(wA), _f64(wB)
+            capi.check(lib().ps_model_ab_set_fields(self._h, capi.dptr(wA), capi.dptr(wB)))
+        return self
+
+    def update(self, n=1):
+        capi.check(lib().ps_model_ab_update(self._h, int(n)))
+
+    def update_timed(self, n):
+        """update(n) timed with CUDA events on the context stream; returns
+        (total_ms, propagator_ms) after synchronising."""
+        tot, prop = ctypes.c_double(), ctypes.c_double()
+        capi.check(lib().ps_model_ab_update_timed(self._h, int(n), ctypes.byref(tot), ctypes.byref(prop)))
+        return tot.value, prop.value
+
+    def propagate(self, n=1):
+        capi.check(lib().ps_model_ab_propagate(self._h, int(n)))
+
+    def synchronize(self):
+        capi.check(lib().ps_model_ab_synchronize(self._h))
+
+    def H(self):
+        H, Hw, Hs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        capi.check(lib().ps_model_ab_H(self._h, ctypes.byref(H), ctypes.byref(Hw), ctypes.byref(Hs)))
+        return H.value, Hw.value, Hs.value
+
+    def residual_error(self):
+        r = ctypes.c_double()
+        capi.check(lib().ps_model_ab_residual(self._h, ctypes.byref(r)))
+        return r.value
+
+    def Q(self):
+        q = ctypes.c_double()
+        capi.check(lib().ps_model_ab_Q(self._h, ctypes.byref(q)))
+        return q.value
+
+    def get(self, name):
+        idx = FIELDS[name]
+        if name in ("qA", "qAc"):
+            out = np.zeros((self.Ms[0],) + self.shape)
+        elif name in ("qB", "qBc"):
+            out = np.zeros((self.Ms[1],) + self.shape)
+        else:
+            out = np.zeros(self.shape)
+        capi.check(lib().ps_model_ab_get(self._h, idx, capi.dptr(out)))
+        return out
+
+    def device_ptr(self, name):
+        p = ctypes.c_void_p()
+        capi.check(lib().ps_model_ab_device_ptr(self._h, FIELDS[name], ctypes.byref(p)))
+        return p.value
+
+    def launches_per_iteration(self):
+        return lib().ps_model_ab_launches_per_iteration(self._h)
+
+    def launches_per_propagate(self):
+        return lib().ps_model_ab_launches_per_propagate(self._h)
+
+    def stream(self):
+        return lib().ps_model_ab_stream(self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().ps_model_ab_destroy(h)
+            self._h = None

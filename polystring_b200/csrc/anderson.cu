@@ -1,0 +1,271 @@
+// anderson.cu -- Anderson mixing of the A and B fields kept on the device
+// (restates FieldAX, src/FieldAX.cc:152-427, as driven by Model_AB::update,
+// src/Model_AB.cc:206-253).
+//
+// History layout per field: w(i), d(i), i = 0..n, each M doubles; the ring
+// position cur and the iteration count k live in device memory (AXState) so
+// that one SCFT iteration can be captured once in a CUDA graph and replayed.
+//
+// Per iteration:
+//   ax_prepare  d(cur) = w_target - w(cur) for A and B       (update_d)
+//   ax_dots     partial sums of d(cur) . d(find_index(j)), j = 0..nn
+//   ax_solve    B shift + new row (update_B), U = UA + UB, V = VA + VB,
+//               C = U^-1 V by Gaussian elimination with partial pivoting,
+//               ramp 1 - lambda^(k+1), ring position update     (one block)
+//   ax_combine  W = w(cur) + sum C (w(kk) - w(cur)), D likewise,
+//               w(cur') = W + ramp D, plus the next Boltzmann factors
+#include "ps_internal.h"
+#include "field_kernels.h"
+#include "anderson.h"
+
+namespace ps {
+
+namespace {
+
+__device__ __forceinline__ int find_index(int cur, int n, int j) {
+    int i = j + cur;
+    if (i > n) i -= (n + 1);
+    return i;
+}
+
+// yita / eta and d(cur) for both fields
+__global__ void ax_prepare_kernel(AXArgs a) {
+    const AXState* s = a.state;
+    const int cur = s->cur;
+    const long M = a.M;
+    double* dA = a.dA + (long)cur * M;
+    double* dB = a.dB + (long)cur * M;
+    const double* wA = a.wA + (long)cur * M;
+    const double* wB = a.wB + (long)cur * M;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
+        double pa = a.phiA[i], pb = a.phiB[i];
+        double y;
+        if (a.compressible) {
+            y = a.lamYita * (pa + pb - 1.0);
+        } else {
+            y = 0.5 * (a.dataA[i] + a.dataB[i] - a.chiN);
+            a.yita[i] = y;
+        }
+        dA[i] = (a.chiN * pb + y) - wA[i];
+        dB[i] = (a.chiN * pa + y) - wB[i];
+    }
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kRedThreads) ax_dots_kernel(AXArgs a, double* partial) {
+    const AXState* s = a.state;
+    const int n = s->n, cur = s->cur;
+    const int nn = s->k < n ? s->k : n;
+    const long M = a.M;
+    const double* dcA = a.dA + (long)cur * M;
+    const double* dcB = a.dB + (long)cur * M;
+    double acc[2 * NMAX];
+#pragma unroll
+    for (int j = 0; j < 2 * NMAX; j++) acc[j] = 0.0;
+    long kk[NMAX];
+#pragma unroll
+    for (int j = 0; j < NMAX; j++) kk[j] = (long)find_index(cur, n, j <= nn ? j : 0) * M;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
+        double xa = dcA[i], xb = dcB[i];
+#pragma unroll
+        for (int j = 0; j < NMAX; j++) {
+            if (j <= nn) {
+                acc[j] += xa * a.dA[kk[j] + i];
+                acc[NMAX + j] += xb * a.dB[kk[j] + i];
+            }
+        }
+    }
+    // block reduction
+    __shared__ double sh[2 * NMAX][kRedThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 2 * NMAX; j++) {
+        double v = acc[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[j][warp] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 2 * NMAX; j += blockDim.x) {
+        double t = 0.0;
+        for (int w = 0; w < kRedThreads / 32; w++) t += sh[j][w];
+        partial[(long)blockIdx.x * 2 * NMAX + j] = t;
+    }
+}
+
+// Gaussian elimination with partial pivoting, identical in order to the
+// oracle's orc_solve_small.  Returns 0, or -1 on an exactly zero pivot.
+__device__ int solve_small(int n, double* A, double* b, double* C) {
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double best = fabs(A[k * n + k]);
+        for (int i = k + 1; i < n; i++) {
+            double v = fabs(A[i * n + k]);
+            if (v > best) { best = v; p = i; }
+        }
+        if (best == 0.0) return -1;
+        if (p != k) {
+            for (int j = 0; j < n; j++) { double t = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = t; }
+            double t = b[k]; b[k] = b[p]; b[p] = t;
+        }
+        double piv = A[k * n + k];
+        for (int i = k + 1; i < n; i++) {
+            double f = A[i * n + k] / piv;
+            A[i * n + k] = 0.0;
+            for (int j = k + 1; j < n; j++) A[i * n + j] -= f * A[k * n + j];
+            b[i] -= f * b[k];
+        }
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double s = b[i];
+        for (int j = i + 1; j < n; j++) s -= A[i * n + j] * C[j];
+        C[i] = s / A[i * n + i];
+    }
+    return 0;
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kRedThreads) ax_solve_kernel(AXArgs a, const double* partial, int G) {
+    AXState* s = a.state;
+    const int n = s->n;
+    const int N1 = n + 1;
+    const int nn = s->k < n ? s->k : n;
+    __shared__ double row[2 * NMAX];
+    // fixed-order reduction of the partial sums
+    for (int j = threadIdx.x; j < 2 * NMAX; j += blockDim.x) {
+        double t = 0.0;
+        for (int b = 0; b < G; b++) t += partial[(long)b * 2 * NMAX + j];
+        row[j] = t / (double)a.M;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double* BA = a.BA;
+    double* BB = a.BB;
+    // update_B (FieldAX.cc:321-345): shift, new row 0, symmetrise
+    for (int i = n; i >= 1; i--)
+        for (int j = n; j >= i; j--) {
+            BA[i * N1 + j] = BA[(i - 1) * N1 + (j - 1)];
+            BB[i * N1 + j] = BB[(i - 1) * N1 + (j - 1)];
+        }
+    for (int j = 0; j <= nn; j++) {
+        BA[j] = row[j];
+        BB[j] = row[NMAX + j];
+    }
+    for (int i = 0; i < N1; i++)
+        for (int j = i + 1; j < N1; j++) {
+            BA[j * N1 + i] = BA[i * N1 + j];
+            BB[j * N1 + i] = BB[i * N1 + j];
+        }
+    // U = UA + UB, V = VA + VB (FieldAX.cc:352-381)
+    double U[NMAX * NMAX], V[NMAX], C[NMAX];
+    for (int i = 0; i < nn; i++) {
+        for (int j = 0; j < nn; j++) {
+            double ua = BA[0] - BA[(i + 1) * N1] - BA[j + 1] + BA[(i + 1) * N1 + (j + 1)];
+            double ub = BB[0] - BB[(i + 1) * N1] - BB[j + 1] + BB[(i + 1) * N1 + (j + 1)];
+            U[i * nn + j] = 0.0 + ua + ub;
+        }
+        V[i] = 0.0 + (BA[0] - BA[(i + 1) * N1]) + (BB[0] - BB[(i + 1) * N1]);
+    }
+    int nc = 0;
+    if (nn > 0) {
+        if (solve_small(nn, U, V, C) != 0) {
+            s->status |= 1;
+            for (int i = 0; i < nn; i++) C[i] = 0.0;
+        }
+        nc = nn;
+    }
+    for (int i = 0; i < nc; i++) s->C[i] = C[i];
+    s->nc = nc;
+    s->rampA = 1.0 - pow(s->lamA, (double)(s->k + 1));
+    s->rampB = 1.0 - pow(s->lamB, (double)(s->k + 1));
+    s->cur_old = s->cur;
+    s->cur_new = s->cur > 0 ? s->cur - 1 : n;
+    s->cur = s->cur_new;
+    s->k += 1;
+}
+
+__global__ void ax_combine_kernel(AXArgs a) {
+    const AXState* s = a.state;
+    const int n = s->n, co = s->cur_old, cn = s->cur_new, nc = s->nc;
+    const long M = a.M;
+    __shared__ double C[kAXMaxHist];
+    __shared__ long kk[kAXMaxHist];
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        C[i] = s->C[i];
+        kk[i] = (long)find_index(co, n, i + 1) * M;
+    }
+    __syncthreads();
+    const double rA = s->rampA, rB = s->rampB;
+    const long oc = (long)co * M, on = (long)cn * M;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
+        double wc = a.wA[oc + i], dc = a.dA[oc + i];
+        double W = wc, D = dc;
+        for (int j = 0; j < nc; j++) {
+            W += C[j] * (a.wA[kk[j] + i] - wc);
+            D += C[j] * (a.dA[kk[j] + i] - dc);
+        }
+        double na = W + rA * D;
+        wc = a.wB[oc + i]; dc = a.dB[oc + i];
+        W = wc; D = dc;
+        for (int j = 0; j < nc; j++) {
+            W += C[j] * (a.wB[kk[j] + i] - wc);
+            D += C[j] * (a.dB[kk[j] + i] - dc);
+        }
+        double nb = W + rB * D;
+        a.wA[on + i] = na;
+        a.wB[on + i] = nb;
+        a.dataA[i] = na;
+        a.dataB[i] = nb;
+        if (a.eFA) {
+            a.eFA[i] = exp(-0.5 * a.dsA * na);
+            a.eHA[i] = exp(-0.25 * a.dsA * na);
+            a.eFB[i] = exp(-0.5 * a.dsB * nb);
+            a.eHB[i] = exp(-0.25 * a.dsB * nb);
+        }
+    }
+}
+
+int grid_for(long M) {
+    long g = (M + 255) / 256;
+    if (g > 148L * 8) g = 148L * 8;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+}  // namespace
+
+int ax_nmax(int n) {
+    if (n + 1 <= 8) return 8;
+    if (n + 1 <= 16) return 16;
+    if (n + 1 <= 32) return 32;
+    return 0;
+}
+
+void launch_anderson(const AXArgs& a, double* partial, cudaStream_t st) {
+    const int nmax = ax_nmax(a.n);
+    if (nmax == 0) throw Error(-2, "Anderson history longer than 31 is not supported");
+    ax_prepare_kernel<<<grid_for(a.M), 256, 0, st>>>(a);
+    PS_CUDA(cudaGetLastError());
+    switch (nmax) {
+    case 8:
+        ax_dots_kernel<8><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_solve_kernel<8><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
+        break;
+    case 16:
+        ax_dots_kernel<16><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_solve_kernel<16><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
+        break;
+    default:
+        ax_dots_kernel<32><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_solve_kernel<32><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
+        break;
+    }
+    PS_CUDA(cudaGetLastError());
+    ax_combine_kernel<<<grid_for(a.M), 256, 0, st>>>(a);
+    PS_CUDA(cudaGetLastError());
+}
+
+}  // namespace ps

@@ -1,0 +1,169 @@
+// engine.h -- host-side engine of the polystring_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <vector>
+
+#include "ps_internal.h"
+#include "anderson.h"
+
+namespace ps {
+
+// RAII device array of doubles
+struct DevBuf {
+    double* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void alloc(size_t count);
+    void release();
+    double2* c() const { return reinterpret_cast<double2*>(p); }
+};
+
+// Unit cell (UnitCell.cc:149-296): reciprocal shape matrix g and lengths l
+struct Cell {
+    int dim = 3, system = 0;
+    double a = 0, b = 0, c = 0, alpha = 0, beta = 0, gamma = 0;
+    double g[9] = {0};
+    double l[3] = {0};
+};
+void cell_init(Cell& c);   // throws on bad parameters
+
+// -k^2 on an orthogonal cell (UnitCell.cc:368-418)
+std::vector<double> k2_orthogonal(const Cell& c, int Lx, int Ly, int Lz);
+// exp(-ds |q|^2), 27-image minimum (UnitCell.cc:321-359)
+std::vector<double> k_laplacian(const Cell& c, int Lx, int Ly, int Lz, double ds);
+
+// Line-pass plan of a grid: the axes longer than one, innermost first.
+struct AxisPlan {
+    int naxes = 0;
+    LineGeom ax[3];
+};
+AxisPlan make_axis_plan(int Lx, int Ly, int Lz);
+
+enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1 };
+
+// Which Boltzmann factors a lane uses at step t: set 0 before switch_t,
+// set 1 from switch_t on (a chain crossing the A/B junction).
+struct LaneFactors {
+    const double* eF[2];
+    const double* eH[2];
+    int switch_t;
+    const double* F(int t) const { return t < switch_t ? eF[0] : eF[1]; }
+    const double* H(int t) const { return t < switch_t ? eH[0] : eH[1]; }
+};
+
+// Work space and pass sequence for two real chains advanced together in one
+// packed complex field.  Histories hold (nsteps + 1) slices of M doubles.
+class PairChain {
+public:
+    PairChain(int Lx, int Ly, int Lz, int scheme, int nbatch);
+    // RQM4: L1 = exp(ds k2), L2 = exp(ds k2 / 2); OS2: L1 = exp(-ds q^2)
+    void set_tables(const std::vector<double>& L1, const std::vector<double>& L2);
+    // batched tables: nbatch consecutive tables of M values each
+    void set_tables_batched(const std::vector<double>& L1, const std::vector<double>& L2);
+    // c_in_fixed / c_out_fixed: lane c reads and writes fixed slices instead
+    // of a history (single-chain solves)
+    void enqueue(double* hf, double* hc, long hist_bstride, int nsteps, const LaneFactors& lf,
+                 const LaneFactors& lc, long fac_bstride, cudaStream_t st, const double* c_in_fixed = nullptr,
+                 double* c_out_fixed = nullptr);
+    // kernel launches per pair step
+    int launches_per_step() const;
+    long M() const { return M_; }
+    const AxisPlan& plan() const { return plan_; }
+
+private:
+    int Lx_, Ly_, Lz_, scheme_, nbatch_;
+    long M_;
+    AxisPlan plan_;
+    DevBuf z_[3], u_[2], L1_, L2_;
+    bool batched_tables_ = false;
+};
+
+// Model_AB on the device (Model_AB.cc:85-371 for a periodic cell)
+struct ModelABParams {
+    int dim, Lx, Ly, Lz;
+    Cell cell;
+    int sA, sB;
+    double chiN, lamA, lamB, lamYita;
+    int mde, scft, n_anderson, compressible, contour;
+};
+
+class ModelAB {
+public:
+    explicit ModelAB(const ModelABParams& p);
+    ~ModelAB();
+    void set_fields(const double* wA, const double* wB, bool device_ptrs);
+    void update(int n);
+    // update() with CUDA events around the whole run and around every
+    // propagator-graph replay; after synchronising returns the total device
+    // time (ms) and sets *prop_ms to the summed propagator time
+    double update_timed(int n, double* prop_ms);
+    // replay only the propagator sweeps (the four Propagator::update calls)
+    void propagate(int n);
+    void H(double* H, double* Hw, double* Hs);
+    double residual();
+    double Q();
+    void get(int which, double* out, bool device_dst);
+    double* device_ptr(int which);
+    void sync();
+    cudaStream_t stream() const { return st_; }
+    int launches_per_iteration() const { return launches_per_iter_; }
+    int launches_per_propagate() const { return launches_per_prop_; }
+    long M() const { return M_; }
+    int Ns() const { return Ns_; }
+    long iterations() const { return iter_; }
+    int status();
+
+private:
+    void enqueue_propagate();
+    void enqueue_post();
+    void ensure_graphs();
+    void init_anderson(const double* wA, const double* wB, bool device_ptrs);
+    ModelABParams p_;
+    long M_;
+    int LA_, LB_, Ns_;
+    double dsA_, dsB_;
+    int ruleA_, ruleB_;
+    PairChain* chain_ = nullptr;
+    cudaStream_t st_ = nullptr;
+    cudaGraphExec_t gprop_ = nullptr, gpost_ = nullptr;
+    DevBuf hf_, hc_, wA_, wB_, yita_, phiA_, phiB_, eFA_, eHA_, eFB_, eHB_;
+    DevBuf cA_, cB_, scal_, partial_;
+    // Anderson
+    DevBuf hwA_, hdA_, hwB_, hdB_, BA_, BB_;
+    AXState* axs_ = nullptr;
+    long iter_ = 0;
+    bool fields_set_ = false;
+    int launches_per_iter_ = 0;
+    int launches_per_prop_ = 0;
+};
+
+// Single propagator updater behind the Updater C-ABI (RQM4 / OS2)
+class UpdaterCtx {
+public:
+    UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, double ds);
+    ~UpdaterCtx();
+    UpdaterCtx* clone() const;
+    void solve_device(const double* w, double* qs, int len, cudaStream_t st);
+    void solve_host(const double* w, double* qs, int len);
+    int scheme() const { return scheme_; }
+
+private:
+    int scheme_, Lx_, Ly_, Lz_;
+    Cell cell_;
+    double ds_;
+    long M_;
+    PairChain* chain_ = nullptr;
+    DevBuf eF_, eH_, zero_, scratch_, dw_, dqs_;
+    cudaStream_t st_ = nullptr;
+};
+
+// contour weights c_s of a rule (Simpson.cc, Quadrature4.cc, Density.cc);
+// returns false when the rule's precondition fails
+bool contour_weights(int rule, int n, std::vector<double>& c);
+
+}  // namespace ps

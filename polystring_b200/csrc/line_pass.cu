@@ -1,0 +1,428 @@
+// line_pass.cu -- shared-memory Stockham line FFTs over one axis of a
+// periodic grid, with the elementwise work of the propagator step fused into
+// the first and last passes.
+//
+// A pass works on tiles of T lines of length N.  A tile is staged in shared
+// memory "line fastest" (element n of line l at buf[n * LP + l]) so that
+// consecutive threads touch consecutive lines: the global loads are
+// coalesced for both contiguous lines (innermost axis, S == 1, the tile is one
+// contiguous block) and strided lines (outer axes, the T lines of a tile are
+// contiguous for every n).  Radix passes ping-pong between two tile buffers.
+//
+// The step being computed is the reference's RQM4 / OS2 split step
+// (RQM4.cc:66-92, PseudoSpectral.cc:248-260)
+//     q' = e^{-w h/2} F^-1[ exp(-h k^2) F[ e^{-w h/2} q ] ] / M
+// for two independent real chains packed into one complex field (lane f in
+// the real part, lane c in the imaginary part).  Both lanes share the k-space
+// table, which is real and even in k, so the packed transform carries both
+// real transforms exactly.
+#include "ps_internal.h"
+#include "fft_core.cuh"
+
+namespace ps {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct TileAddr {
+    long base, nstride, lstride;
+};
+
+__device__ __forceinline__ TileAddr tile_addr(const LineGeom& g, long tile) {
+    long l0 = tile * g.T;
+    TileAddr a;
+    if (g.S == 1) {
+        a.base = l0 * g.N; a.nstride = 1; a.lstride = g.N;
+    } else {
+        long o = l0 / g.S, i0 = l0 % g.S;
+        a.base = o * (long)g.N * g.S + i0; a.nstride = g.S; a.lstride = 1;
+    }
+    return a;
+}
+
+// element e of a tile -> (n, line); global offset; smem index
+struct Elem {
+    int n, l;
+    long goff;
+    int sidx;
+};
+
+__device__ __forceinline__ Elem elem(const LineGeom& g, const TileAddr& a, int e) {
+    Elem r;
+    if (g.S == 1) { r.l = e / g.N; r.n = e - r.l * g.N; }
+    else          { r.n = e / g.T; r.l = e - r.n * g.T; }
+    r.goff = a.base + (long)r.n * a.nstride + (long)r.l * a.lstride;
+    r.sidx = r.n * g.LP + r.l;
+    return r;
+}
+
+template <int N, int R, int NS, int SIGN>
+__device__ __forceinline__ void run_pass(const double2* in, double2* out, int T, int LP, const double2* tw) {
+    const int total = T * (N / R);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        int j = b / T;
+        int l = b - j * T;
+        butterfly<N, R, NS, SIGN>(in, out, LP, l, j, tw);
+    }
+}
+
+// Full line FFT of the tile held in A (B is the ping-pong partner).  Returns
+// the buffer that holds the result.  Caller synchronises before the call.
+template <int N, int SIGN>
+__device__ __forceinline__ double2* tile_fft(double2* A, double2* B, int T, int LP, const double2* tw) {
+    using P = Plan<N>;
+    if constexpr (P::P >= 1) { run_pass<N, P::r0, 1, SIGN>(A, B, T, LP, tw); __syncthreads(); }
+    if constexpr (P::P >= 2) { run_pass<N, P::r1, P::r0, SIGN>(B, A, T, LP, tw); __syncthreads(); }
+    if constexpr (P::P >= 3) { run_pass<N, P::r2, P::r0 * P::r1, SIGN>(A, B, T, LP, tw); __syncthreads(); }
+    return (P::P % 2 == 1) ? B : A;
+}
+
+__device__ __forceinline__ double2* other(double2* r, double2* A, double2* B) { return r == A ? B : A; }
+
+template <int N, int MODE>
+__global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtrs p, const double2* __restrict__ gtw) {
+    extern __shared__ double2 smem[];
+    double2* twf = smem;
+    double2* twi = smem + N;
+    const int tile_elems = N * g.LP;
+    double2* A = smem + 2 * N;
+    double2* B = A + tile_elems;
+    double2* C = B + tile_elems;   // END / FULL modes: chain values (lane f, lane c)
+    double2* D = C + tile_elems;   // FULL RQM4: full-step result u
+
+    for (int m = threadIdx.x; m < N; m += blockDim.x) {
+        double2 t = gtw[m];
+        twf[m] = t;
+        twi[m] = make_double2(t.x, -t.y);
+    }
+
+    const long tile = blockIdx.x;
+    const int fy = blockIdx.y;
+    const long bz = blockIdx.z;
+    const TileAddr ta = tile_addr(g, tile);
+    const int nel = N * g.T;
+    const double M = p.M;
+
+    const long oz = bz * p.bstride_z, oq = bz * p.bstride_q, oe = bz * p.bstride_e, oL = bz * p.bstride_L;
+    const long ou = bz * p.bstride_u;
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_OUTER) {
+        double2* z = p.z[fy] + oz;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            A[el.sidx] = z[el.goff];
+        }
+        __syncthreads();
+        double2* r;
+        if constexpr (MODE == MODE_INV) {
+            r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
+        } else {
+            r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+        }
+        if constexpr (MODE == MODE_OUTER) {
+            const double* L = p.L[fy] + oL;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double lv = L[el.goff];
+                double2 v = r[el.sidx];
+                r[el.sidx] = make_double2(v.x * lv, v.y * lv);
+            }
+            __syncthreads();
+            r = tile_fft<N, +1>(r, other(r, A, B), g.T, g.LP, twi);
+        }
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            z[el.goff] = r[el.sidx];
+        }
+    } else if constexpr (MODE == MODE_FIRST_RQM4 || MODE == MODE_FIRST_OS2) {
+        // Z = (e_f q_f) + i (e_c q_c); RQM4: y = 0 uses e^{-w ds/2} (full
+        // step), y = 1 uses e^{-w ds/4} (first half step).
+        const double* ef = (fy == 0 ? p.eF[0] : p.eH[0]) + oe;
+        const double* ec = (fy == 0 ? p.eF[1] : p.eH[1]) + oe;
+        const double* qf = p.qin[0] + oq;
+        const double* qc = p.qin[1] + oq;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            A[el.sidx] = make_double2(ef[el.goff] * qf[el.goff], ec[el.goff] * qc[el.goff]);
+        }
+        __syncthreads();
+        double2* r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+        double2* z = p.z[fy] + oz;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            z[el.goff] = r[el.sidx];
+        }
+    } else if constexpr (MODE == MODE_MID_RQM4) {
+        if (fy == 0) {
+            // full step: u = Re/Im(F^-1 Z1) e^{-w ds/2} / M
+            double2* z = p.z[0] + oz;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                A[el.sidx] = z[el.goff];
+            }
+            __syncthreads();
+            double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
+            const double* ef = p.eF[0] + oe;
+            const double* ec = p.eF[1] + oe;
+            double* uf = p.u[0] + ou;
+            double* uc = p.u[1] + ou;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double2 v = r[el.sidx];
+                uf[el.goff] = (v.x * ef[el.goff]) / M;
+                uc[el.goff] = (v.y * ec[el.goff]) / M;
+            }
+        } else {
+            // first half step finishes, second half step starts
+            double2* z = p.z[1] + oz;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                A[el.sidx] = z[el.goff];
+            }
+            __syncthreads();
+            double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
+            const double* hf = p.eH[0] + oe;
+            const double* hc = p.eH[1] + oe;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double2 v = r[el.sidx];
+                double a = hf[el.goff], b = hc[el.goff];
+                double qtf = (v.x * a) / M;
+                double qtc = (v.y * b) / M;
+                r[el.sidx] = make_double2(a * qtf, b * qtc);
+            }
+            __syncthreads();
+            double2* r2 = tile_fft<N, -1>(r, other(r, A, B), g.T, g.LP, twf);
+            double2* z3 = p.z[2] + oz;
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                z3[el.goff] = r2[el.sidx];
+            }
+        }
+    } else if constexpr (MODE == MODE_END_RQM4 || MODE == MODE_END_OS2) {
+        double2* zin = (MODE == MODE_END_RQM4 ? p.z[2] : p.z[0]) + oz;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            A[el.sidx] = zin[el.goff];
+        }
+        __syncthreads();
+        double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
+        const double* hf = (MODE == MODE_END_RQM4 ? p.eH[0] : p.eF[0]) + oe;
+        const double* hc = (MODE == MODE_END_RQM4 ? p.eH[1] : p.eF[1]) + oe;
+        double* of = p.qout[0] + oq;
+        double* oc = p.qout[1] + oq;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            double2 v = r[el.sidx];
+            double qf = (v.x * hf[el.goff]) / M;
+            double qc = (v.y * hc[el.goff]) / M;
+            if constexpr (MODE == MODE_END_RQM4) {
+                qf = (4.0 * qf - p.u[0][ou + el.goff]) / 3.0;
+                qc = (4.0 * qc - p.u[1][ou + el.goff]) / 3.0;
+            }
+            of[el.goff] = qf;
+            oc[el.goff] = qc;
+            C[el.sidx] = make_double2(qf, qc);
+        }
+        if (p.chain_next) {
+            const int nz = (MODE == MODE_END_RQM4) ? 2 : 1;
+            for (int k = 0; k < nz; k++) {
+                const double* nf = (k == 0 ? p.nF[0] : p.nH[0]) + oe;
+                const double* nc = (k == 0 ? p.nF[1] : p.nH[1]) + oe;
+                __syncthreads();
+                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                    Elem el = elem(g, ta, e);
+                    double2 q = C[el.sidx];
+                    A[el.sidx] = make_double2(nf[el.goff] * q.x, nc[el.goff] * q.y);
+                }
+                __syncthreads();
+                double2* r2 = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+                double2* z = p.z[k] + oz;
+                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                    Elem el = elem(g, ta, e);
+                    z[el.goff] = r2[el.sidx];
+                }
+            }
+        }
+    } else if constexpr (MODE == MODE_FULL_RQM4 || MODE == MODE_FULL_OS2) {
+        // single-axis grids: the whole step inside one tile
+        const double* qf = p.qin[0] + oq;
+        const double* qc = p.qin[1] + oq;
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            C[el.sidx] = make_double2(qf[el.goff], qc[el.goff]);
+        }
+        const double* ef = p.eF[0] + oe;
+        const double* ec = p.eF[1] + oe;
+        const double* L1 = p.L[0] + oL;
+        // sub-step 1: full ds step
+        __syncthreads();
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            double2 q = C[el.sidx];
+            A[el.sidx] = make_double2(ef[el.goff] * q.x, ec[el.goff] * q.y);
+        }
+        __syncthreads();
+        double2* r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+            Elem el = elem(g, ta, e);
+            double lv = L1[el.goff];
+            double2 v = r[el.sidx];
+            r[el.sidx] = make_double2(v.x * lv, v.y * lv);
+        }
+        __syncthreads();
+        r = tile_fft<N, +1>(r, other(r, A, B), g.T, g.LP, twi);
+        double* of = p.qout[0] + oq;
+        double* oc = p.qout[1] + oq;
+        if constexpr (MODE == MODE_FULL_OS2) {
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double2 v = r[el.sidx];
+                of[el.goff] = (v.x * ef[el.goff]) / M;
+                oc[el.goff] = (v.y * ec[el.goff]) / M;
+            }
+        } else {
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double2 v = r[el.sidx];
+                D[el.sidx] = make_double2((v.x * ef[el.goff]) / M, (v.y * ec[el.goff]) / M);
+            }
+            const double* hf = p.eH[0] + oe;
+            const double* hc = p.eH[1] + oe;
+            const double* L2 = p.L[1] + oL;
+            // two ds/2 steps: start from C, keep the intermediate in C
+            for (int h = 0; h < 2; h++) {
+                __syncthreads();
+                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                    Elem el = elem(g, ta, e);
+                    double2 q = C[el.sidx];
+                    A[el.sidx] = make_double2(hf[el.goff] * q.x, hc[el.goff] * q.y);
+                }
+                __syncthreads();
+                r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                    Elem el = elem(g, ta, e);
+                    double lv = L2[el.goff];
+                    double2 v = r[el.sidx];
+                    r[el.sidx] = make_double2(v.x * lv, v.y * lv);
+                }
+                __syncthreads();
+                r = tile_fft<N, +1>(r, other(r, A, B), g.T, g.LP, twi);
+                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                    Elem el = elem(g, ta, e);
+                    double2 v = r[el.sidx];
+                    C[el.sidx] = make_double2((v.x * hf[el.goff]) / M, (v.y * hc[el.goff]) / M);
+                }
+            }
+            __syncthreads();
+            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+                Elem el = elem(g, ta, e);
+                double2 q = C[el.sidx];
+                double2 u = D[el.sidx];
+                of[el.goff] = (4.0 * q.x - u.x) / 3.0;
+                oc[el.goff] = (4.0 * q.y - u.y) / 3.0;
+            }
+        }
+    }
+}
+
+constexpr int kMaxSmem = 200 * 1024;
+
+int buffers_for_mode(int mode) {
+    switch (mode) {
+    case MODE_END_RQM4: case MODE_END_OS2: case MODE_FULL_OS2: return 3;
+    case MODE_FULL_RQM4: return 4;
+    default: return 2;
+    }
+}
+
+int grid_y_for_mode(int mode, int nfield) {
+    switch (mode) {
+    case MODE_FWD: case MODE_INV: case MODE_OUTER: return nfield;
+    case MODE_FIRST_RQM4: case MODE_MID_RQM4: return 2;
+    default: return 1;
+    }
+}
+
+template <int N, int MODE>
+void prepare_nm() {
+    PS_CUDA(cudaFuncSetAttribute(line_pass_kernel<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kMaxSmem));
+}
+
+template <int N, int MODE>
+void launch_nm(const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st, bool prepare_only) {
+    if (prepare_only) { prepare_nm<N, MODE>(); return; }
+    size_t smem = line_pass_smem_bytes(MODE, g);
+    if (smem > (size_t)kMaxSmem) throw Error(-2, "line pass tile does not fit in shared memory");
+    dim3 grid((unsigned)g.ntiles, (unsigned)grid_y_for_mode(MODE, p.nfield), (unsigned)nbatch);
+    line_pass_kernel<N, MODE><<<grid, kThreads, smem, st>>>(g, p, twiddle_table(N));
+    PS_CUDA(cudaGetLastError());
+}
+
+template <int N>
+void launch_n(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st, bool po) {
+    switch (mode) {
+    case MODE_FWD: launch_nm<N, MODE_FWD>(g, p, nbatch, st, po); break;
+    case MODE_INV: launch_nm<N, MODE_INV>(g, p, nbatch, st, po); break;
+    case MODE_OUTER: launch_nm<N, MODE_OUTER>(g, p, nbatch, st, po); break;
+    case MODE_FIRST_RQM4: launch_nm<N, MODE_FIRST_RQM4>(g, p, nbatch, st, po); break;
+    case MODE_MID_RQM4: launch_nm<N, MODE_MID_RQM4>(g, p, nbatch, st, po); break;
+    case MODE_END_RQM4: launch_nm<N, MODE_END_RQM4>(g, p, nbatch, st, po); break;
+    case MODE_FIRST_OS2: launch_nm<N, MODE_FIRST_OS2>(g, p, nbatch, st, po); break;
+    case MODE_END_OS2: launch_nm<N, MODE_END_OS2>(g, p, nbatch, st, po); break;
+    case MODE_FULL_RQM4: launch_nm<N, MODE_FULL_RQM4>(g, p, nbatch, st, po); break;
+    case MODE_FULL_OS2: launch_nm<N, MODE_FULL_OS2>(g, p, nbatch, st, po); break;
+    default: throw Error(-1, "unknown line pass mode");
+    }
+}
+
+}  // namespace
+
+bool line_size_supported(int N) {
+    switch (N) {
+    case 2: case 4: case 8: case 12: case 16: case 24: case 32: case 48: case 64:
+    case 96: case 128: case 192: case 256: return true;
+    default: return false;
+    }
+}
+
+namespace {
+void dispatch(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st, bool po) {
+    switch (g.N) {
+    case 2: launch_n<2>(mode, g, p, nbatch, st, po); break;
+    case 4: launch_n<4>(mode, g, p, nbatch, st, po); break;
+    case 8: launch_n<8>(mode, g, p, nbatch, st, po); break;
+    case 12: launch_n<12>(mode, g, p, nbatch, st, po); break;
+    case 16: launch_n<16>(mode, g, p, nbatch, st, po); break;
+    case 24: launch_n<24>(mode, g, p, nbatch, st, po); break;
+    case 32: launch_n<32>(mode, g, p, nbatch, st, po); break;
+    case 48: launch_n<48>(mode, g, p, nbatch, st, po); break;
+    case 64: launch_n<64>(mode, g, p, nbatch, st, po); break;
+    case 96: launch_n<96>(mode, g, p, nbatch, st, po); break;
+    case 128: launch_n<128>(mode, g, p, nbatch, st, po); break;
+    case 192: launch_n<192>(mode, g, p, nbatch, st, po); break;
+    case 256: launch_n<256>(mode, g, p, nbatch, st, po); break;
+    default: throw Error(-2, "unsupported FFT line length " + std::to_string(g.N));
+    }
+}
+}  // namespace
+
+size_t line_pass_smem_bytes(int mode, const LineGeom& g) {
+    return sizeof(double2) * (2 * (size_t)g.N + (size_t)buffers_for_mode(mode) * g.N * g.LP);
+}
+
+void prepare_line_pass(int mode, const LineGeom& g) {
+    StepPtrs p{};
+    dispatch(mode, g, p, 1, 0, true);
+    twiddle_table(g.N);
+    if (line_pass_smem_bytes(mode, g) > (size_t)kMaxSmem)
+        throw Error(-2, "line pass tile does not fit in shared memory");
+}
+
+void launch_line_pass(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st) {
+    dispatch(mode, g, p, nbatch, st, false);
+}
+
+}  // namespace ps

@@ -1,0 +1,90 @@
+// ps_internal.h -- shared declarations of the polystring_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <stdexcept>
+
+namespace ps {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define PS_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess)                                                     \
+            throw ::ps::Error(-3, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// line passes (kernels in line_pass.cu)
+// ---------------------------------------------------------------------------
+enum PassMode {
+    MODE_FWD = 0,        // forward line FFT of every field
+    MODE_INV = 1,        // inverse line FFT of every field
+    MODE_OUTER = 2,      // forward, multiply by the k-space table, inverse
+    MODE_FIRST_RQM4 = 3, // real chain slices -> Z1 (ds step), Z2 (ds/2 step), forward
+    MODE_MID_RQM4 = 4,   // inverse Z1 -> full-step result u; inverse Z2 -> qt -> Z3, forward
+    MODE_END_RQM4 = 5,   // inverse Z3 -> qt2, q = (4 qt2 - u)/3 (+ next step's FIRST)
+    MODE_FIRST_OS2 = 6,  // real chain slices -> Z, forward
+    MODE_END_OS2 = 7,    // inverse Z -> q (+ next step's FIRST)
+    MODE_FULL_RQM4 = 8,  // whole RQM4 step when the grid has a single axis
+    MODE_FULL_OS2 = 9,   // whole OS2 step when the grid has a single axis
+};
+
+// Geometry of one line pass over a (batch of) field(s) of M points.
+struct LineGeom {
+    int N;        // line length (FFT size)
+    long S;       // element stride of a line
+    int T;        // lines per tile
+    int LP;       // smem line pitch (T or T + 1)
+    long nlines;  // lines per field (M / N)
+    long ntiles;  // tiles per field (nlines / T)
+};
+
+// Pointers used by the fused first / last passes.  A "lane" is one of the
+// two real chains packed into one complex field: lane f in the real part,
+// lane c in the imaginary part.
+struct StepPtrs {
+    double2* z[3];           // packed complex work fields W1, W2, W3
+    const double* L[3];      // k-space tables for the OUTER pass of z[i]
+    const double* qin[2];    // real inputs (chain slices s), lanes f, c
+    double* qout[2];         // real outputs (chain slices s + 1)
+    double* u[2];            // RQM4 full-step scratch (lanes f, c)
+    const double* eF[2];     // exp(-w ds / 2) for the current step, per lane
+    const double* eH[2];     // exp(-w ds / 4) (RQM4 half steps), per lane
+    const double* nF[2];     // next step's factors (END modes with chaining)
+    const double* nH[2];
+    int chain_next;          // END modes: also run the next step's FIRST
+    int nfield;              // FWD / INV / OUTER: number of fields in z[]
+    double M;                // grid points (normalisation of the inverse)
+    long bstride_z;          // batch strides (elements) for batched launches
+    long bstride_q;          // history slices (qin / qout)
+    long bstride_u;          // u scratch buffers
+    long bstride_e;          // factor arrays
+    long bstride_L;          // k tables
+};
+
+void launch_line_pass(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st);
+// sets kernel attributes and builds twiddles; call outside stream capture
+void prepare_line_pass(int mode, const LineGeom& g);
+size_t line_pass_smem_bytes(int mode, const LineGeom& g);
+bool line_size_supported(int N);
+
+// ---------------------------------------------------------------------------
+// twiddles
+// ---------------------------------------------------------------------------
+// Device table of W_N^m = exp(-2 pi i m / N) (forward) for a supported N,
+// computed on the host in long double and rounded once.
+const double2* twiddle_table(int N);
+
+}  // namespace ps

@@ -1,0 +1,93 @@
+"""Seeded synthetic inputs of the benchmark configurations.
+
+There is no public dataset on this path; every configuration is an AB
+diblock melt on a periodic cell with fields generated from a seed on the
+host and handed identically to the CUDA path and to the CPU oracle.
+
+  C1  2D 64x64, square 4.0 Rg, fA 0.30, chiN 20, Ns 100 (Ms [31, 71]), RQM4,
+      simple mixing lambda 0.1; w = 0.1 U(-1,1) +/- 0.5 x (6-fold cosine)
+  C2  3D 64^3, cubic 4.2 Rg, fA 0.35, chiN 25, Ns 200 (Ms [71, 131]), RQM4,
+      Anderson (history 20); w = 0.1 N(0,1) +/- 1.0 x (gyroid level set)
+  C3  40 images, 2D 128x128, square 8.0 Rg, fA 0.35, chiN 18, Ns 128
+      (Ms [46, 84], Quad4_Closed on both blocks); images interpolate between
+      a lamellar field (cos x, amp 2.0) and a hexagonal field (3 waves, amp
+      2.0), each plus 0.05 N(0,1)
+  C4  3D 48^3, orthorhombic (3.8, 4.0, 4.2), fA 0.30, chiN 22, Ns 128
+      (Ms [39, 91])
+
+Ms follows from fA and Ns as LA = round(fA Ns), LB = Ns - LA, Ms = [LA+1, LB+1]
+(the reference reads Ms and recomputes f = LA/(LA+LB), src/Model_AB.cc:100-111).
+"""
+import numpy as np
+
+
+def ms_from(fA, Ns):
+    LA = int(round(fA * Ns))
+    return (LA + 1, Ns - LA + 1)
+
+
+def _coords(shape, lengths):
+    axes = []
+    for n, L in zip(shape, lengths):
+        axes.append(np.arange(n) * (L / n))
+    return np.meshgrid(*axes, indexing="ij")
+
+
+def six_fold(shape, L):
+    """Sum of three plane waves at 60 degrees with wavevector 2 pi / L."""
+    x, y = _coords(shape[:2], (L, L))
+    k = 2 * np.pi / L
+    s = np.zeros(shape[:2])
+    for ang in (0.0, np.pi / 3, 2 * np.pi / 3):
+        s += np.cos(k * (np.cos(ang) * x + np.sin(ang) * y))
+    return (s / 3.0).reshape(shape)
+
+
+def gyroid(shape, L):
+    x, y, z = _coords(shape, (L, L, L))
+    k = 2 * np.pi / L
+    return (np.sin(k * x) * np.cos(k * y) + np.sin(k * y) * np.cos(k * z) + np.sin(k * z) * np.cos(k * x))
+
+
+def config(name, seed=2024):
+    """Parameters and initial fields of a configuration (C1, C2, C4)."""
+    rng = np.random.default_rng(seed)
+    if name == "C1":
+        shape, L = (64, 64, 1), 4.0
+        base = 0.1 * rng.uniform(-1, 1, (2,) + shape)
+        c6 = six_fold(shape, L)
+        return dict(dim=2, shape=shape, cell=("SQUARE", (L,)), Ms=ms_from(0.30, 100), chiN=20.0,
+                    lam=(0.1, 0.1, 5.0), mde="RQM4", scft="EM", n_anderson=5, iters=500,
+                    wA=base[0] + 0.5 * c6, wB=base[1] - 0.5 * c6)
+    if name == "C2":
+        shape, L = (64, 64, 64), 4.2
+        base = 0.1 * rng.standard_normal((2,) + shape)
+        g = gyroid(shape, L)
+        return dict(dim=3, shape=shape, cell=("CUBIC", (L,)), Ms=ms_from(0.35, 200), chiN=25.0,
+                    lam=(0.05, 0.05, 5.0), mde="RQM4", scft="Anderson", n_anderson=20, iters=1000,
+                    wA=base[0] + 1.0 * g, wB=base[1] - 1.0 * g)
+    if name == "C4":
+        shape, L = (48, 48, 48), (3.8, 4.0, 4.2)
+        base = 0.1 * rng.standard_normal((2,) + shape)
+        return dict(dim=3, shape=shape, cell=("ORTHORHOMBIC", L), Ms=ms_from(0.30, 128), chiN=22.0,
+                    lam=(0.05, 0.05, 5.0), mde="RQM4", scft="Anderson", n_anderson=20, iters=300,
+                    wA=base[0], wB=base[1])
+    raise KeyError(name)
+
+
+def string_images(m=40, shape=(128, 128, 1), L=8.0, seed=2024):
+    """C3 initial string: m images linearly interpolated between a lamellar
+    and a hexagonal field (polystring_AB.cc:207-214 interpolation)."""
+    rng = np.random.default_rng(seed)
+    x, y = _coords(shape[:2], (L, L))
+    k = 2 * np.pi / L
+    lam = (2.0 * np.cos(k * x)).reshape(shape)
+    hexa = (2.0 * sum(np.cos(k * (np.cos(a) * x + np.sin(a) * y)) for a in (0.0, np.pi / 3, 2 * np.pi / 3)) / 3.0)
+    hexa = hexa.reshape(shape)
+    e0A = lam + 0.05 * rng.standard_normal(shape)
+    e0B = -lam + 0.05 * rng.standard_normal(shape)
+    e1A = hexa + 0.05 * rng.standard_normal(shape)
+    e1B = -hexa + 0.05 * rng.standard_normal(shape)
+    wa = np.stack([e0A + i / (m - 1) * (e1A - e0A) for i in range(m)])
+    wb = np.stack([e0B + i / (m - 1) * (e1B - e0B) for i in range(m)])
+    return wa, wb
