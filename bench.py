@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="only warm-up and timed iterations (for ncu captures); prints a short line")
     return ap.parse_args()
 
 
@@ -124,8 +126,9 @@ class Clocks:
 
 def cpu_baseline(cfg, seconds, threads):
     """Time the CPU oracle (the restatement of the reference's step sequence)
-    on a bounded sample: whole SCFT iterations of the same workload when one
-    fits in the time budget, else contour steps of the forward propagator."""
+    on a bounded sample of the workload: RQM4 contour steps of one 64^3
+    propagator, as many as fit in `seconds` (about 95% of an SCFT iteration
+    is propagation)."""
     import oracle
     oracle.build()
     oracle.set_threads(threads)
@@ -231,6 +234,12 @@ def main():
     barrier()
     torch.cuda.synchronize()
     total_s = allmax(total_ms / 1e3)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "ms_per_step": total_s / args.steps * 1e3,
+                              "propagator_ms_per_step": prop_ms / args.steps,
+                              "launches_per_step": m.launches_per_iteration()}), flush=True)
+        return
     value = world * units_per_step * args.steps / total_s
     launches = m.launches_per_iteration() * args.steps
     H = m.H()[0]

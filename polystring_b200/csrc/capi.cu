@@ -1,6 +1,6 @@
 // capi.cu -- extern "C" entry points declared in include/polystring_b200.h.
 // Every function catches C++ exceptions and maps them to status codes.
-#include "../../include/polystring_b200.h"
+#include "polystring_b200.h"
 #include "engine.h"
 #include "field_kernels.h"
 

@@ -5,6 +5,7 @@
 #include "field_kernels.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 
@@ -384,6 +385,52 @@ ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
         }
         chain_->set_tables(L1, L2);
     }
+    const char* force = getenv("PS_B200_LINE_PASSES");
+    const char* generic = getenv("PS_B200_GENERIC_SWEEP");
+    const bool allow = !(force && force[0] == '1');
+    use_sweep64_ = allow && p.mde == 0 && sweep64_supported(p.Lx, p.Ly, p.Lz) && !(generic && generic[0] == '1');
+    use_sweep_ = allow && p.mde == 0 && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
+    if (use_sweep64_) {
+        sweep_grid_ = sweep64_prepare();
+        swZ_.alloc(6 * (size_t)M_);
+        swU_.alloc(2 * (size_t)M_);
+        // per-axis factors exp(h cc_axis r^2), h = ds (full) and ds/2 (half)
+        const double PI = 3.14159265358979323846;
+        std::vector<double> tab(6 * 64);
+        const int Ls[3] = {p.Lx, p.Ly, p.Lz};
+        for (int half = 0; half < 2; half++)
+            for (int ax = 0; ax < 3; ax++) {
+                double cc = -4.0 * PI * PI / (p_.cell.l[ax] * p_.cell.l[ax]);
+                double h = half ? 0.5 * dsA_ : dsA_;
+                for (int i = 0; i < 64; i++) {
+                    int ri = (i < Ls[ax] / 2 + 1) ? i : Ls[ax] - i;
+                    tab[half * 192 + ax * 64 + i] = exp(h * (cc * ri * ri));
+                }
+            }
+        swTab_.alloc(tab.size());
+        PS_CUDA(cudaMemcpy(swTab_.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMalloc(&swbar_, 64 * sizeof(unsigned)));
+        PS_CUDA(cudaMalloc(&swerr_, sizeof(int)));
+        PS_CUDA(cudaMemset(swerr_, 0, sizeof(int)));
+    }
+    if (use_sweep_) {
+        sweep_grid_ = sweep_prepare(p.Lx, p.Ly, p.Lz);
+        swZ_.alloc(6 * (size_t)M_);
+        swU_.alloc(2 * (size_t)M_);
+        std::vector<double> k2 = k2_orthogonal(p_.cell, p.Lx, p.Ly, p.Lz);
+        std::vector<double> L1(M_), L2(M_);
+        for (long m = 0; m < M_; m++) {
+            L1[m] = exp(dsA_ * k2[m]);
+            L2[m] = exp(0.5 * dsA_ * k2[m]);
+        }
+        swL1_.alloc(M_);
+        swL2_.alloc(M_);
+        PS_CUDA(cudaMemcpy(swL1_.p, L1.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMemcpy(swL2_.p, L2.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMalloc(&swbar_, 32 * sizeof(unsigned)));
+        PS_CUDA(cudaMalloc(&swerr_, sizeof(int)));
+        PS_CUDA(cudaMemset(swerr_, 0, sizeof(int)));
+    }
     hf_.alloc((size_t)(Ns_ + 1) * M_);
     hc_.alloc((size_t)(Ns_ + 1) * M_);
     wA_.alloc(M_); wB_.alloc(M_); yita_.alloc(M_);
@@ -406,7 +453,7 @@ ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
     PS_CUDA(cudaStreamSynchronize(st_));
-    launches_per_prop_ = chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
+    launches_per_prop_ = (use_sweep_ || use_sweep64_) ? 1 : chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
     launches_per_iter_ = launches_per_prop_ + 2 + 2 + (p.scft == 1 ? 4 : 1);
 }
 
@@ -415,6 +462,8 @@ ModelAB::~ModelAB() {
     if (gpost_) cudaGraphExecDestroy(gpost_);
     delete chain_;
     if (axs_) cudaFree(axs_);
+    if (swbar_) cudaFree(swbar_);
+    if (swerr_) cudaFree(swerr_);
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -453,6 +502,32 @@ void ModelAB::set_fields(const double* wA, const double* wB, bool dev) {
 void ModelAB::enqueue_propagate() {
     // propagators: forward chain qA -> qB, complementary chain qBc -> qAc
     // (Model_AB.cc:139-145, 187-193)
+    if (use_sweep64_) {
+        SweepArgs a{};
+        a.hf = hf_.p; a.hc = hc_.p;
+        a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
+        a.uf = swU_.p; a.uc = nullptr;
+        a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
+        a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
+        a.bar = swbar_; a.err = swerr_;
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 64 * sizeof(unsigned), st_));
+        sweep64_launch(a, swTab_.p, sweep_grid_, st_);
+        return;
+    }
+    if (use_sweep_) {
+        SweepArgs a{};
+        a.hf = hf_.p; a.hc = hc_.p;
+        a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
+        a.uf = swU_.p; a.uc = swU_.p + M_;
+        a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
+        a.L1 = swL1_.p; a.L2 = swL2_.p;
+        a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
+        a.bar = swbar_; a.err = swerr_;
+        a.bstride_batch = 0; a.bstride_hist = 0; a.bstride_L = 0;
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), st_));
+        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, st_);
+        return;
+    }
     LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
     LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
     chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, st_);
@@ -605,11 +680,20 @@ double ModelAB::residual() {
 }
 
 int ModelAB::status() {
-    if (!axs_) return 0;
-    AXState s;
-    PS_CUDA(cudaMemcpyAsync(&s, axs_, sizeof(AXState), cudaMemcpyDeviceToHost, st_));
-    PS_CUDA(cudaStreamSynchronize(st_));
-    return s.status;
+    int st = 0;
+    if (axs_) {
+        AXState s;
+        PS_CUDA(cudaMemcpyAsync(&s, axs_, sizeof(AXState), cudaMemcpyDeviceToHost, st_));
+        PS_CUDA(cudaStreamSynchronize(st_));
+        st |= s.status;
+    }
+    if (swerr_) {
+        int e = 0;
+        PS_CUDA(cudaMemcpyAsync(&e, swerr_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        PS_CUDA(cudaStreamSynchronize(st_));
+        if (e) st |= 2;
+    }
+    return st;
 }
 
 double* ModelAB::device_ptr(int which) {

@@ -6,6 +6,7 @@
 
 #include "ps_internal.h"
 #include "anderson.h"
+#include "sweep.h"
 
 namespace ps {
 
@@ -117,6 +118,7 @@ public:
     int Ns() const { return Ns_; }
     long iterations() const { return iter_; }
     int status();
+    bool persistent_sweep() const { return use_sweep_; }
 
 private:
     void enqueue_propagate();
@@ -129,6 +131,13 @@ private:
     double dsA_, dsB_;
     int ruleA_, ruleB_;
     PairChain* chain_ = nullptr;
+    // persistent sweep (RQM4 on the shapes sweep_supported() lists)
+    bool use_sweep_ = false;
+    bool use_sweep64_ = false;
+    int sweep_grid_ = 0;
+    DevBuf swZ_, swU_, swL1_, swL2_, swTab_;
+    unsigned* swbar_ = nullptr;
+    int* swerr_ = nullptr;
     cudaStream_t st_ = nullptr;
     cudaGraphExec_t gprop_ = nullptr, gpost_ = nullptr;
     DevBuf hf_, hc_, wA_, wB_, yita_, phiA_, phiB_, eFA_, eHA_, eFB_, eHB_;

@@ -1,0 +1,33 @@
+// sweep.h -- persistent cooperative RQM4 sweep of a paired chain.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ps {
+
+struct SweepArgs {
+    double *hf, *hc;                 // histories, (Ns + 1) x M each (slice 0 = head)
+    double2 *Z1, *Z2, *Z3;           // packed complex work fields, M each
+    double *uf, *uc;                 // full-step results, M each
+    const double *eFA, *eHA, *eFB, *eHB;   // Boltzmann factors of the A and B blocks
+    const double *L1, *L2;           // exp(ds k2), exp(ds k2 / 2)
+    const double2 *twx, *twy, *twz;  // twiddles (set by the launcher)
+    int LA, LB, Ns;
+    unsigned* bar;                   // one barrier counter per problem (stride 32), zeroed per launch
+    int* err;                        // nonzero after a barrier timeout
+    long bstride_batch;              // per-problem stride of M-sized arrays
+    long bstride_hist;               // per-problem stride of the histories
+    long bstride_L;                  // per-problem stride of the k tables (0: shared)
+};
+
+bool sweep_supported(int Lx, int Ly, int Lz);
+// 64^3 specialisation (sweep64.cu); bar needs 64 zeroed words, uf holds the
+// interleaved (u_f, u_c) pairs (2 M doubles); tables = 6 x 64 per-axis k factors
+bool sweep64_supported(int Lx, int Ly, int Lz);
+int sweep64_prepare();
+void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStream_t st);
+// sets kernel attributes, builds twiddles; returns the cooperative grid size
+int sweep_prepare(int Lx, int Ly, int Lz);
+void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st);
+
+}  // namespace ps

@@ -188,3 +188,72 @@ def test_published_free_energy_2d(ps, golden, mde, scft, tag):
     assert r < 1e-6
     # the 2D runs stopped at residual 1e-6: H is pinned to that level
     assert abs(m.H()[0] - F_tab[i]) < 1e-6, (m.H()[0], F_tab[i])
+
+
+@pytest.mark.parametrize("shape,L", [((32, 32, 32), (3.6, 3.8, 4.0)), ((48, 48, 48), (3.8, 4.0, 4.2)),
+                                     ((64, 64, 64), (4.2, 4.2, 4.2))])
+@pytest.mark.parametrize("scft", ["EM", "Anderson"])
+def test_persistent_sweep_matches_oracle(ps, shape, L, scft):
+    """3D grids that run the persistent cooperative sweep (one launch per
+    propagator sweep) against the oracle, short chains."""
+    oracle.set_threads(oracle.max_threads())
+    o, m = _models(ps, 3, shape, L, (9, 13), 20.0, scft=scft, n_anderson=3)
+    assert m.launches_per_propagate() == 1
+    wA, wB = _seed_fields(shape, 21)
+    o.init_fields(wA, wB)
+    m.set_fields(wA, wB)
+    for n in (1, 2):
+        o.update(n)
+        m.update(n)
+        assert abs(m.Q() - o.Q()) / o.Q() < 1e-10
+        assert abs(m.H()[0] - o.H()[0]) / abs(o.H()[0]) < 1e-10
+        for f in ("phiA", "phiB", "wA", "wB"):
+            assert np.abs(m.get(f) - o.get(f)).max() < 1e-10, f
+    for f in ("qA", "qB", "qAc", "qBc"):
+        assert _rel(m.get(f), o.get(f)) < 1e-12, f
+
+
+def test_full_size_chain_symmetry(ps):
+    """At the full 64^3, Ns = 200 size: the RQM4 step operator is symmetric,
+    so mean(q_N) of the forward chain equals mean(q^dagger_N) of the
+    complementary chain; and densities integrate to fA, fB within the
+    contour quadrature error."""
+    from polystring_b200 import workloads
+    cfg = workloads.config("C2")
+    cell = ps.make_cell(3, "CUBIC", cfg["cell"][1][0])
+    m = ps.ModelAB(3, cfg["shape"], cell, cfg["Ms"], cfg["chiN"], lam=cfg["lam"], scft="Anderson", n_anderson=20)
+    m.set_fields(cfg["wA"], cfg["wB"])
+    for _ in range(3):
+        m.update(1)
+        qB = m.get("qB")[-1]
+        qAc = m.get("qAc")[-1]
+        assert abs(qB.mean() - qAc.mean()) / qB.mean() < 1e-12
+        fa = m.get("phiA").mean()
+        fb = m.get("phiB").mean()
+        assert abs(fa + fb - 1.0) < 1e-6
+        assert abs(fa - 70.0 / 200.0) < 1e-3
+
+
+@pytest.mark.parametrize("engine", ["sweep64", "generic", "line_passes"])
+def test_64cube_engines_agree_with_oracle(ps, engine, monkeypatch):
+    """The three GPU code paths for a 64^3 grid (specialised persistent sweep,
+    generic persistent sweep, per-pass launches) against the oracle."""
+    if engine == "generic":
+        monkeypatch.setenv("PS_B200_GENERIC_SWEEP", "1")
+    if engine == "line_passes":
+        monkeypatch.setenv("PS_B200_LINE_PASSES", "1")
+    oracle.set_threads(oracle.max_threads())
+    shape = (64, 64, 64)
+    o, m = _models(ps, 3, shape, (4.2, 4.2, 4.2), (11, 17), 25.0, scft="Anderson", n_anderson=4)
+    assert (m.launches_per_propagate() == 1) == (engine != "line_passes")
+    wA, wB = _seed_fields(shape, 8)
+    o.init_fields(wA, wB)
+    m.set_fields(wA, wB)
+    o.update(2)
+    m.update(2)
+    assert abs(m.Q() - o.Q()) / o.Q() < 1e-10
+    assert abs(m.H()[0] - o.H()[0]) / abs(o.H()[0]) < 1e-10
+    for f in ("phiA", "phiB", "wA", "wB"):
+        assert np.abs(m.get(f) - o.get(f)).max() < 1e-10, f
+    for f in ("qA", "qB", "qAc", "qBc"):
+        assert _rel(m.get(f), o.get(f)) < 1e-12, f
