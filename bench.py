@@ -64,7 +64,7 @@ def peaks():
 def traffic_per_gridpt_step():
     """DRAM bytes per gridpoint-step of the propagator line passes from the
     committed ncu summary (None until one exists)."""
-    path = os.path.join(ROOT, "profiles", "propagator_line_passes_64cube.txt")
+    path = os.path.join(ROOT, "profiles", "propagator_sweep64_c2_64cube.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -272,7 +272,7 @@ def main():
     tr = traffic_per_gridpt_step()
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": tr * units_per_step if tr else None, "peak_kind": peak_kind,
-            "kernel": "propagator sweep (line-pass kernels), %d launches per iteration" % m.launches_per_propagate(),
+            "kernel": "propagator sweep (persistent RQM4 kernel), %d launch(es) per iteration" % m.launches_per_propagate(),
             "propagator_share_of_step": prop_s / total_s}
 
     cpu = None

@@ -115,12 +115,13 @@ __device__ __forceinline__ bool mbar_wait(void* bar, unsigned parity) {
 }
 
 // ---- 64-point four-step FFT, 8 lanes per line ----------------------------
+// tw8[k1 * 8 + t] = W64^(t k1): lanes t = 0..7 read consecutive entries
 template <int SIGN>
-__device__ __forceinline__ void pass1(double2 (&v)[8], int t, const double2* tw) {
+__device__ __forceinline__ void pass1(double2 (&v)[8], int t, const double2* tw8) {
     Dft<8, SIGN>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < 8; k1++) {
-        double2 w = tw[(t * k1) & 63];
+        double2 w = tw8[k1 * 8 + t];
         if (SIGN > 0) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     unsigned bidx = 0;
     unsigned mphase = 0;
 
-    for (int i = tid; i < 64; i += NT) tw[i] = a.twx[i];
+    for (int i = tid; i < 64; i += NT) tw[i] = a.twx[((i & 7) * (i >> 3)) & 63];   // [k1][t]
     for (int i = tid; i < 6 * 64; i += NT) tab[i] = tables[i];
     if (planar) {
         for (int i = tid; i < P64; i += NT) {
@@ -259,7 +260,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     if (tid == 0) mbar_init(mbar);
     __syncthreads();
 
-    const int gwarp = b * (NT / 32) + (tid >> 5);
+    // x-pass warp index, CTA-fastest so that a phase's tasks spread over all SMs
+    const int gwarp = (tid >> 5) * gridDim.x + b;
     const int nwarps = gridDim.x * (NT / 32);
     double2* Z1 = a.Z1;
     double2* Z2 = a.Z2;
@@ -290,9 +292,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     for (int st = 0; st < a.Ns; st++) {
         // ---- x-pass on Z1 (full step) and Z2 (half step) ---------------------
         {
-            const int half = (gwarp >= nwarps / 2) ? 1 : 0;
-            const int w0 = half ? gwarp - nwarps / 2 : gwarp;
-            xpass(half ? Z2 : Z1, half, s, w0, nwarps / 2);
+            const int half = gwarp & 1;
+            xpass(half ? Z2 : Z1, half, s, gwarp >> 1, nwarps >> 1);
         }
         if (!grid_sync(ctr, a.err, ++bidx)) return;
 
