@@ -168,6 +168,30 @@ int ps_model_ab_launches_per_propagate(ps_model_ab* m);
 /* CUDA stream of the context (cudaStream_t as void*) */
 void* ps_model_ab_stream(ps_model_ab* m);
 
+/* ---- string method: all images of the string on the device ----------- */
+typedef struct ps_string_ab ps_string_ab;
+/* polystring_AB (scft/polystring_AB.cc:111-152) with m images of the model
+ * in p (p->scft must be PS_SCFT_EM: images restart from DATA_INIT fields,
+ * Model_AB.cc:52-83) and max_iter SCFT iterations per image per string
+ * iteration ([Algorithm_SCFT] max_iter).  3 <= m <= 64. */
+int ps_string_ab_create(const ps_model_ab_params* p, int m, int max_iter, ps_string_ab** out);
+void ps_string_ab_destroy(ps_string_ab* s);
+/* initial string, m x M per field, image-major (initialize_string,
+ * polystring_AB.cc:184-222); images 0 and m-1 are the fixed ends */
+int ps_string_ab_set_images(ps_string_ab* s, const double* wa, const double* wb);
+/* n string iterations: SCFT of every image (run_scftInString :256-281),
+ * arc length (parameterize_string :283-296), per-point natural cubic spline
+ * re-sampling and end restoration (redistribute_stringBeads :298-329) */
+int ps_string_ab_iterate(ps_string_ab* s, int n);
+/* H of every image after the last iteration (m values) */
+int ps_string_ab_H(ps_string_ab* s, double* H);
+/* normalised arc length of every image (m values) */
+int ps_string_ab_S(ps_string_ab* s, double* S);
+/* which: 0 wa, 1 wb, 2 phiA, 3 phiB; m x M values */
+int ps_string_ab_get(ps_string_ab* s, int which, double* out);
+int ps_string_ab_synchronize(ps_string_ab* s);
+int ps_string_ab_launches_per_iteration(ps_string_ab* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -305,3 +305,23 @@ def string_redistribute(f, S, end0, end1):
     rc = lib().orc_string_redistribute(_p(f), _p(S), m, M, _p(e0), _p(e1))
     assert rc == 0
     return f
+
+
+def string_iteration(model, wa, wb, end_a, end_b, max_iter):
+    """One iteration of polystring_AB (scft/polystring_AB.cc:125-150) on the
+    CPU: every image restarts from its fields (fresh Yita, resetInString) and
+    runs max_iter updates; then arc length from wa, per-point natural spline
+    re-sampling of wa and wb, ends restored.  wa, wb (m, ...) are updated in
+    place; returns (H per image, S)."""
+    m = wa.shape[0]
+    H = np.zeros(m)
+    for s in range(m):
+        model.init_fields(wa[s], wb[s])
+        model.update(max_iter)
+        H[s] = model.H()[0]
+        wa[s] = model.get("wA")
+        wb[s] = model.get("wB")
+    S = string_arclength(wa)
+    string_redistribute(wa, S, end_a[0], end_a[1])
+    string_redistribute(wb, S, end_b[0], end_b[1])
+    return H, S

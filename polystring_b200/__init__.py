@@ -197,3 +197,65 @@ class ModelAB:
         if h:
             lib().ps_model_ab_destroy(h)
             self._h = None
+
+
+class StringAB:
+    """polystring_AB on the device: m images advanced together, one captured
+    graph per string iteration (SCFT of every image, arc length, spline
+    re-sampling, ends restored)."""
+
+    def __init__(self, m, dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", max_iter=3,
+                 compressible=False, contour="Simpson"):
+        Lx, Ly, Lz = shape
+        p = capi.ModelABParamsC()
+        p.dim, p.Lx, p.Ly, p.Lz = dim, Lx, Ly, Lz
+        p.cell = cell
+        p.sA, p.sB = Ms
+        p.chiN = chiN
+        p.lamA, p.lamB, p.lamYita = lam
+        p.mde = capi.MDE[mde.upper()]
+        p.scft = 0
+        p.n_anderson = 1
+        p.compressible = 1 if compressible else 0
+        p.contour = capi.CONTOUR[contour.upper()]
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_string_ab_create(ctypes.byref(p), int(m), int(max_iter), ctypes.byref(h)))
+        self._h = h
+        self.m = m
+        self.shape = tuple(shape)
+
+    def set_images(self, wa, wb):
+        wa, wb = _f64(wa), _f64(wb)
+        capi.check(lib().ps_string_ab_set_images(self._h, capi.dptr(wa), capi.dptr(wb)))
+        return self
+
+    def iterate(self, n=1):
+        capi.check(lib().ps_string_ab_iterate(self._h, int(n)))
+
+    def synchronize(self):
+        capi.check(lib().ps_string_ab_synchronize(self._h))
+
+    def H(self):
+        out = np.zeros(self.m)
+        capi.check(lib().ps_string_ab_H(self._h, capi.dptr(out)))
+        return out
+
+    def S(self):
+        out = np.zeros(self.m)
+        capi.check(lib().ps_string_ab_S(self._h, capi.dptr(out)))
+        return out
+
+    def get(self, name):
+        idx = {"wa": 0, "wb": 1, "phiA": 2, "phiB": 3}[name]
+        out = np.zeros((self.m,) + self.shape)
+        capi.check(lib().ps_string_ab_get(self._h, idx, capi.dptr(out)))
+        return out
+
+    def launches_per_iteration(self):
+        return lib().ps_string_ab_launches_per_iteration(self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().ps_string_ab_destroy(h)
+            self._h = None

@@ -77,6 +77,16 @@ SIGNATURES = [
     ("ps_model_ab_launches_per_iteration", ctypes.c_int, [_vp]),
     ("ps_model_ab_launches_per_propagate", ctypes.c_int, [_vp]),
     ("ps_model_ab_stream", _vp, [_vp]),
+    ("ps_string_ab_create", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(_vp)]),
+    ("ps_string_ab_destroy", None, [_vp]),
+    ("ps_string_ab_set_images", ctypes.c_int, [_vp, _dp, _dp]),
+    ("ps_string_ab_iterate", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("ps_string_ab_H", ctypes.c_int, [_vp, _dp]),
+    ("ps_string_ab_S", ctypes.c_int, [_vp, _dp]),
+    ("ps_string_ab_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    ("ps_string_ab_synchronize", ctypes.c_int, [_vp]),
+    ("ps_string_ab_launches_per_iteration", ctypes.c_int, [_vp]),
 ]
 
 _lib = None

@@ -3,6 +3,7 @@
 #include "polystring_b200.h"
 #include "engine.h"
 #include "field_kernels.h"
+#include "string_ab.h"
 
 #include <string>
 #include <vector>
@@ -52,6 +53,7 @@ using namespace ps;
 
 struct ps_updater { UpdaterCtx* ctx; };
 struct ps_model_ab { ModelAB* ctx; };
+struct ps_string_ab { StringAB* ctx; };
 
 extern "C" {
 
@@ -138,21 +140,26 @@ int ps_grid_mean_device(const double* x, long long M, double* out_host, void* st
     });
 }
 
+static ModelABParams to_params(const ps_model_ab_params* p) {
+    if (!p) throw Error(PS_ERR_INVALID, "null parameters");
+    check_dims(p->dim, p->Lx, p->Ly, p->Lz);
+    if (p->cell.dim != p->dim) throw Error(PS_ERR_INVALID, "cell dimension differs from grid dimension");
+    if (p->mde != PS_MDE_RQM4 && p->mde != PS_MDE_OS2) throw Error(PS_ERR_INVALID, "unknown MDE scheme");
+    if (p->scft != PS_SCFT_EM && p->scft != PS_SCFT_ANDERSON) throw Error(PS_ERR_INVALID, "unknown SCFT algorithm");
+    ModelABParams q;
+    q.dim = p->dim; q.Lx = p->Lx; q.Ly = p->Ly; q.Lz = p->Lz;
+    q.cell = to_cell(&p->cell);
+    q.sA = p->sA; q.sB = p->sB; q.chiN = p->chiN;
+    q.lamA = p->lamA; q.lamB = p->lamB; q.lamYita = p->lamYita;
+    q.mde = p->mde; q.scft = p->scft; q.n_anderson = p->n_anderson;
+    q.compressible = p->compressible; q.contour = p->contour;
+    return q;
+}
+
 int ps_model_ab_create(const ps_model_ab_params* p, ps_model_ab** out) {
     return guarded([&] {
         if (!p || !out) throw Error(PS_ERR_INVALID, "null argument");
-        check_dims(p->dim, p->Lx, p->Ly, p->Lz);
-        if (p->cell.dim != p->dim) throw Error(PS_ERR_INVALID, "cell dimension differs from grid dimension");
-        if (p->mde != PS_MDE_RQM4 && p->mde != PS_MDE_OS2) throw Error(PS_ERR_INVALID, "unknown MDE scheme");
-        if (p->scft != PS_SCFT_EM && p->scft != PS_SCFT_ANDERSON) throw Error(PS_ERR_INVALID, "unknown SCFT algorithm");
-        ModelABParams q;
-        q.dim = p->dim; q.Lx = p->Lx; q.Ly = p->Ly; q.Lz = p->Lz;
-        q.cell = to_cell(&p->cell);
-        q.sA = p->sA; q.sB = p->sB; q.chiN = p->chiN;
-        q.lamA = p->lamA; q.lamB = p->lamB; q.lamYita = p->lamYita;
-        q.mde = p->mde; q.scft = p->scft; q.n_anderson = p->n_anderson;
-        q.compressible = p->compressible; q.contour = p->contour;
-        *out = new ps_model_ab{new ModelAB(q)};
+        *out = new ps_model_ab{new ModelAB(to_params(p))};
     });
 }
 
@@ -244,5 +251,62 @@ int ps_model_ab_launches_per_iteration(ps_model_ab* m) { return m ? m->ctx->laun
 int ps_model_ab_launches_per_propagate(ps_model_ab* m) { return m ? m->ctx->launches_per_propagate() : -1; }
 
 void* ps_model_ab_stream(ps_model_ab* m) { return m ? (void*)m->ctx->stream() : nullptr; }
+
+int ps_string_ab_create(const ps_model_ab_params* p, int m, int max_iter, ps_string_ab** out) {
+    return guarded([&] {
+        if (!p || !out) throw Error(PS_ERR_INVALID, "null argument");
+        *out = new ps_string_ab{new StringAB(to_params(p), m, max_iter)};
+    });
+}
+
+void ps_string_ab_destroy(ps_string_ab* s) {
+    if (!s) return;
+    delete s->ctx;
+    delete s;
+}
+
+int ps_string_ab_set_images(ps_string_ab* s, const double* wa, const double* wb) {
+    return guarded([&] {
+        if (!s || !wa || !wb) throw Error(PS_ERR_INVALID, "null argument");
+        s->ctx->set_images(wa, wb, false);
+    });
+}
+
+int ps_string_ab_iterate(ps_string_ab* s, int n) {
+    return guarded([&] {
+        if (!s) throw Error(PS_ERR_INVALID, "null handle");
+        s->ctx->iterate(n);
+    });
+}
+
+int ps_string_ab_H(ps_string_ab* s, double* H) {
+    return guarded([&] {
+        if (!s || !H) throw Error(PS_ERR_INVALID, "null argument");
+        s->ctx->H(H);
+    });
+}
+
+int ps_string_ab_S(ps_string_ab* s, double* S) {
+    return guarded([&] {
+        if (!s || !S) throw Error(PS_ERR_INVALID, "null argument");
+        s->ctx->S(S);
+    });
+}
+
+int ps_string_ab_get(ps_string_ab* s, int which, double* out) {
+    return guarded([&] {
+        if (!s || !out) throw Error(PS_ERR_INVALID, "null argument");
+        s->ctx->get(which, out, false);
+    });
+}
+
+int ps_string_ab_synchronize(ps_string_ab* s) {
+    return guarded([&] {
+        if (!s) throw Error(PS_ERR_INVALID, "null handle");
+        s->ctx->sync();
+    });
+}
+
+int ps_string_ab_launches_per_iteration(ps_string_ab* s) { return s ? s->ctx->launches_per_iteration() : -1; }
 
 }  // extern "C"

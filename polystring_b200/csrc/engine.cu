@@ -236,7 +236,7 @@ void PairChain::enqueue(double* hf, double* hc, long hist_bstride, int nsteps, c
     const long M = M_;
     StepPtrs base{};
     base.M = (double)M;
-    base.bstride_z = 2 * M;
+    base.bstride_z = M;         // in double2 elements
     base.bstride_q = hist_bstride;
     base.bstride_u = M;
     base.bstride_e = fac_bstride;

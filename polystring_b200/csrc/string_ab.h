@@ -1,0 +1,43 @@
+// string_ab.h -- batched string method context (string_ab.cu).
+#pragma once
+
+#include "engine.h"
+
+namespace ps {
+
+constexpr int kMaxImages = 64;   // images per string (spline arrays live in registers/local memory)
+
+class StringAB {
+public:
+    StringAB(const ModelABParams& p, int m, int max_iter);
+    ~StringAB();
+    // wa, wb: m x M (image-major); the first and last images are the ends
+    void set_images(const double* wa, const double* wb, bool device_ptrs);
+    void iterate(int n);                 // n string iterations (graph replays)
+    void H(double* out);                 // free energy of every image (last iteration)
+    void S(double* out);                 // normalised arc length of every image
+    void get(int which, double* out, bool device_dst);   // 0 wa, 1 wb, 2 phiA, 3 phiB (m x M)
+    void sync();
+    int images() const { return m_; }
+    long M() const { return M_; }
+    int Ns() const { return Ns_; }
+    int launches_per_iteration() const;
+    cudaStream_t stream() const { return st_; }
+
+private:
+    void enqueue_scft_iteration();
+    void enqueue_string_iteration();
+    ModelABParams p_;
+    int m_, max_iter_;
+    long M_;
+    int LA_, LB_, Ns_;
+    double dsA_, dsB_;
+    PairChain* chain_ = nullptr;
+    cudaStream_t st_ = nullptr;
+    cudaGraphExec_t giter_ = nullptr;
+    DevBuf hf_, hc_, wa_, wb_, yita_, phiA_, phiB_, eFA_, eHA_, eFB_, eHB_, ends_, cA_, cB_, scal_, S_, partial_;
+    long iters_ = 0;
+    bool ready_ = false;
+};
+
+}  // namespace ps
