@@ -65,9 +65,29 @@ def build(force=False, verbose=False, jobs=None):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB + ".tmp"] + objs
         subprocess.check_call(cmd)
         os.replace(LIB + ".tmp", LIB)
+    build_host(force)
     if verbose:
         print("".join(logs))
     return LIB
+
+
+HOST_SRC = ["polyorder.cc", "polyorder_b200.cc"]
+HOST_EXE = os.path.join(BUILD, "polyorder_b200")
+
+
+def build_host(force=False):
+    """The C++ host classes and the polyorder_b200 driver, linked against
+    libpolystring_b200.so (g++, rpath to the library's directory)."""
+    host = os.path.join(HERE, "host")
+    srcs = [os.path.join(host, f) for f in HOST_SRC]
+    deps = srcs + [os.path.join(host, "polyorder.h"), LIB] + _headers()
+    if not force and not _needs(HOST_EXE, deps):
+        return HOST_EXE
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), "-o", HOST_EXE + ".tmp"] + srcs + \
+        ["-L", BUILD, "-lpolystring_b200", "-Wl,-rpath,$ORIGIN"]
+    subprocess.check_call(cmd)
+    os.replace(HOST_EXE + ".tmp", HOST_EXE)
+    return HOST_EXE
 
 
 if __name__ == "__main__":

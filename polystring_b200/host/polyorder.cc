@@ -1,0 +1,506 @@
+// polyorder.cc -- implementation of the host classes in polyorder.h.
+#include "polyorder.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <random>
+#include <sstream>
+
+namespace polyorder {
+
+namespace {
+
+std::string lower(std::string s) {
+    std::transform(s.begin(), s.end(), s.begin(), [](unsigned char c) { return (char)std::tolower(c); });
+    return s;
+}
+std::string upper(std::string s) {
+    std::transform(s.begin(), s.end(), s.begin(), [](unsigned char c) { return (char)std::toupper(c); });
+    return s;
+}
+std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+    return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+void check(int rc) {
+    if (rc != PS_OK) throw std::runtime_error(std::string("polystring_b200: ") + ps_last_error());
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Config (INI sections/keys are case-insensitive, as SimpleIni's default)
+// ---------------------------------------------------------------------------
+Config::Config(const std::string& file) {
+    std::ifstream in(file);
+    if (!in) throw std::runtime_error("cannot open config file " + file);
+    size_t slash = file.find_last_of('/');
+    dir_ = slash == std::string::npos ? std::string("./") : file.substr(0, slash + 1);
+    std::string line, section;
+    while (std::getline(in, line)) {
+        std::string t = trim(line);
+        if (t.empty() || t[0] == '#' || t[0] == ';') continue;
+        if (t[0] == '[') {
+            size_t e = t.find(']');
+            section = lower(trim(t.substr(1, e == std::string::npos ? std::string::npos : e - 1)));
+            continue;
+        }
+        size_t eq = t.find('=');
+        if (eq == std::string::npos) continue;
+        kv_[section][lower(trim(t.substr(0, eq)))] = trim(t.substr(eq + 1));
+    }
+}
+
+std::string Config::get_string(const std::string& section, const std::string& key, const std::string& def) const {
+    auto s = kv_.find(lower(section));
+    if (s == kv_.end()) return def;
+    auto k = s->second.find(lower(key));
+    if (k == s->second.end() || k->second.empty()) return def;
+    return k->second;
+}
+
+double Config::get_double(const std::string& section, const std::string& key, double def) const {
+    std::string v = get_string(section, key);
+    return v.empty() ? def : std::stod(v);
+}
+
+int Config::get_integer(const std::string& section, const std::string& key, int def) const {
+    std::string v = get_string(section, key);
+    return v.empty() ? def : (int)std::stol(v);
+}
+
+bool Config::get_bool(const std::string& section, const std::string& key, bool def) const {
+    std::string v = lower(get_string(section, key));
+    if (v.empty()) return def;
+    return v == "true" || v == "1" || v == "yes" || v == "on";
+}
+
+// Python-style lists "[a, b, c]" (Config.cc:1549-1624)
+std::vector<double> Config::get_list(const std::string& section, const std::string& key) const {
+    std::string v = get_string(section, key);
+    std::vector<double> out;
+    std::string cur;
+    for (char ch : v) {
+        if (ch == '[' || ch == ']' || ch == ',' || ch == ' ') {
+            if (!trim(cur).empty()) out.push_back(std::stod(trim(cur)));
+            cur.clear();
+        } else {
+            cur += ch;
+        }
+    }
+    if (!trim(cur).empty()) out.push_back(std::stod(trim(cur)));
+    return out;
+}
+
+void Config::set(const std::string& section, const std::string& key, double v) {
+    std::ostringstream os;
+    os << std::setprecision(17) << v;
+    kv_[lower(section)][lower(key)] = os.str();
+}
+
+// Config::algo_mde_type (Config.cc:1099-1111)
+AlgorithmMDEType Config::algo_mde_type() const {
+    std::string t = upper(get_string("Algorithm_MDE", "algorithm"));
+    if (t == "PSEUDOSPECTRAL" || t == "OS2" || t == "OS") return AlgorithmMDEType::OS2;
+    if (t == "RQM4" || t == "OS4") return AlgorithmMDEType::RQM4;
+    return AlgorithmMDEType::ETDRK4;
+}
+
+// Config::algo_scft_type (Config.cc:1219-1235)
+AlgorithmSCFTType Config::algo_scft_type() const {
+    std::string t = upper(get_string("Algorithm_SCFT", "algorithm"));
+    if (t == "ANDERSON" || t == "ANDERSON_MIXING" || t == "ANDERSON MIXING") return AlgorithmSCFTType::ANDERSON;
+    return AlgorithmSCFTType::EM;
+}
+
+// Config::algo_contour_integration_type (Config.cc:1495-1505)
+AlgorithmContourType Config::algo_contour_integration_type() const {
+    std::string t = upper(get_string("Algorithm_Contour_Integration", "algorithm"));
+    if (t == "TRAPEZOIDAL" || t == "TRAP" || t == "TRAPE" || t == "TRAPZ") return AlgorithmContourType::TRAPEZOIDAL;
+    return AlgorithmContourType::SIMPSON;
+}
+
+// Config::algo_cell_optimization_type (Config.cc:1335-1349)
+AlgorithmCellType Config::algo_cell_optimization_type() const {
+    std::string t = upper(get_string("Algorithm_Cell_Optimization", "algorithm"));
+    if (t == "MANUAL" || t == "BATCH") return AlgorithmCellType::MANUAL;
+    if (t == "BRENT" || t == "BRENT METHOD" || t == "NEWTON") return AlgorithmCellType::BRENT;
+    return AlgorithmCellType::SINGLE;
+}
+
+// Config::get_grid_init_type (Config.cc:977-992)
+GridInitType Config::get_grid_init_type() const {
+    std::string t = upper(get_string("Grid", "gridInitType"));
+    if (t == "CONST" || t == "CONSTANT") return GridInitType::CONSTANT_INIT;
+    if (t == "DATA") return GridInitType::DATA_INIT;
+    if (t == "FILE") return GridInitType::FILE_INIT;
+    if (t == "PATTERN") return GridInitType::PATTERN_INIT;
+    return GridInitType::RANDOM_INIT;
+}
+
+// ---------------------------------------------------------------------------
+// UnitCell (crystal system names of Config::get_crystal_system_type, :518-547)
+// ---------------------------------------------------------------------------
+UnitCell::UnitCell(const Config& cfg) {
+    std::memset(&cell_, 0, sizeof(cell_));
+    cell_.dim = cfg.dim();
+    std::string t = upper(cfg.crystal_system());
+    int sys = -1;
+    if (t == "LAM" || t == "LAMELLAR" || t == "LAMELLA" || t == "LAMELLAE") sys = PS_CELL_LAMELLAR;
+    else if (t == "SQUARE" || t == "SQ") sys = PS_CELL_SQUARE;
+    else if (t == "RECT" || t == "RECTANGLE" || t == "RECTANGULAR") sys = PS_CELL_RECTANGULAR;
+    else if (t == "HEX" || t == "HEXAGONAL" || t == "HEXGON") sys = cell_.dim == 3 ? PS_CELL_HEXAGONAL3 : PS_CELL_HEXAGONAL2;
+    else if (t == "OBLIQUE" || t == "OB") sys = PS_CELL_OBLIQUE;
+    else if (t == "CUBIC" || t == "CUBE") sys = PS_CELL_CUBIC;
+    else if (t == "TETRAGONAL" || t == "TETRAGON") sys = PS_CELL_TETRAGONAL;
+    else if (t == "ORTHORHOMBIC") sys = PS_CELL_ORTHORHOMBIC;
+    else if (t == "TRIGONAL") sys = PS_CELL_TRIGONAL;
+    else if (t == "MONOCLINIC") sys = PS_CELL_MONOCLINIC;
+    else if (t == "TRICLINIC") sys = PS_CELL_TRICLINIC;
+    if (sys < 0) throw std::runtime_error("unknown crystal system type: " + cfg.crystal_system());
+    cell_.system = sys;
+    cell_.a = cfg.a();
+    cell_.b = cfg.b();
+    cell_.c = cfg.c();
+    cell_.alpha = cfg.get_double("UnitCell", "alpha");
+    cell_.beta = cfg.get_double("UnitCell", "beta");
+    cell_.gamma = cfg.get_double("UnitCell", "gamma");
+    if (sys == PS_CELL_SQUARE || sys == PS_CELL_HEXAGONAL2) cell_.b = cell_.a;
+    if (sys == PS_CELL_CUBIC) { cell_.b = cell_.a; cell_.c = cell_.a; }
+    if (sys == PS_CELL_TETRAGONAL || sys == PS_CELL_HEXAGONAL3) cell_.b = cell_.a;
+}
+
+// ---------------------------------------------------------------------------
+// Grid and MAT-file v5
+// ---------------------------------------------------------------------------
+double Grid::quadrature() const {
+    double s = 0.0;
+    for (double v : data_) s += v;
+    return s / (double)data_.size();
+}
+
+namespace {
+constexpr uint32_t miINT8 = 1, miINT32 = 5, miUINT32 = 6, miDOUBLE = 9, miMATRIX = 14;
+
+struct Rd {
+    const std::vector<char>& b;
+    size_t off;
+    uint32_t u32(size_t o) const { uint32_t v; std::memcpy(&v, b.data() + o, 4); return v; }
+};
+
+// one data element: type, byte count, payload offset, total size (padded)
+void tag(const std::vector<char>& b, size_t off, uint32_t& type, uint32_t& nbytes, size_t& data, size_t& total) {
+    uint32_t w0;
+    std::memcpy(&w0, b.data() + off, 4);
+    if (w0 >> 16) {   // small data element
+        type = w0 & 0xffff;
+        nbytes = w0 >> 16;
+        data = off + 4;
+        total = 8;
+    } else {
+        type = w0;
+        std::memcpy(&nbytes, b.data() + off + 4, 4);
+        data = off + 8;
+        total = 8 + ((nbytes + 7) / 8) * 8;
+    }
+}
+}  // namespace
+
+std::vector<double> mat_read(const std::string& file, const std::string& name, std::vector<int>* dims_out) {
+    std::ifstream in(file, std::ios::binary);
+    if (!in) throw std::runtime_error("cannot open MAT-file " + file);
+    std::vector<char> b((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    if (b.size() < 128) throw std::runtime_error("truncated MAT-file " + file);
+    size_t off = 128;
+    while (off + 8 <= b.size()) {
+        uint32_t type, nb;
+        size_t data, total;
+        tag(b, off, type, nb, data, total);
+        if (data + nb > b.size()) throw std::runtime_error("truncated MAT-file " + file);
+        if (type == 15) throw std::runtime_error("compressed MAT-files are not supported: " + file);
+        if (type == miMATRIX) {
+            size_t p = data, end = data + nb;
+            uint32_t t, n;
+            size_t d, tot;
+            tag(b, p, t, n, d, tot);          // array flags
+            p += tot;
+            tag(b, p, t, n, d, tot);          // dimensions
+            std::vector<int> dims(n / 4);
+            for (size_t i = 0; i < dims.size(); i++) { int32_t v; std::memcpy(&v, b.data() + d + 4 * i, 4); dims[i] = v; }
+            p += tot;
+            tag(b, p, t, n, d, tot);          // name
+            std::string vname(b.data() + d, n);
+            p += tot;
+            if (vname == name) {
+                tag(b, p, t, n, d, tot);      // real part
+                if (t != miDOUBLE || p + tot > end) throw std::runtime_error("variable " + name + " is not a double array");
+                std::vector<double> v(n / 8);
+                std::memcpy(v.data(), b.data() + d, n);
+                if (dims_out) *dims_out = dims;
+                return v;
+            }
+        }
+        off += total;
+    }
+    throw std::runtime_error("variable " + name + " not found in " + file);
+}
+
+void mat_write(const std::string& file, const std::map<std::string, std::pair<std::vector<int>, std::vector<double>>>& vars) {
+    std::ofstream out(file, std::ios::binary);
+    if (!out) throw std::runtime_error("cannot write MAT-file " + file);
+    char hdr[128];
+    std::memset(hdr, ' ', 116);
+    std::snprintf(hdr, 116, "MATLAB 5.0 MAT-file, written by polystring_b200");
+    hdr[std::strlen(hdr)] = ' ';
+    std::memset(hdr + 116, 0, 8);
+    uint16_t ver = 0x0100;
+    std::memcpy(hdr + 124, &ver, 2);
+    hdr[126] = 'I';
+    hdr[127] = 'M';
+    out.write(hdr, 128);
+    auto w32 = [&](uint32_t v) { out.write(reinterpret_cast<const char*>(&v), 4); };
+    for (const auto& kv : vars) {
+        const std::string& nm = kv.first;
+        const std::vector<int>& dims = kv.second.first;
+        const std::vector<double>& v = kv.second.second;
+        uint32_t name_pad = ((uint32_t)nm.size() + 7) / 8 * 8;
+        uint32_t dim_bytes = 4 * (uint32_t)dims.size(), dim_pad = (dim_bytes + 7) / 8 * 8;
+        uint32_t body = 16 + 8 + dim_pad + 8 + name_pad + 8 + 8 * (uint32_t)v.size();
+        w32(miMATRIX); w32(body);
+        w32(miUINT32); w32(8); w32(6); w32(0);                  // mxDOUBLE_CLASS
+        w32(miINT32); w32(dim_bytes);
+        for (int d : dims) w32((uint32_t)d);
+        for (uint32_t i = dim_bytes; i < dim_pad; i++) out.put(0);
+        w32(miINT8); w32((uint32_t)nm.size());
+        out.write(nm.data(), nm.size());
+        for (uint32_t i = (uint32_t)nm.size(); i < name_pad; i++) out.put(0);
+        w32(miDOUBLE); w32(8 * (uint32_t)v.size());
+        out.write(reinterpret_cast<const char*>(v.data()), 8 * v.size());
+    }
+}
+
+// MAT stores column-major (Fortran) order; the grid is row-major (z fastest)
+void Grid::load_mat(const std::string& file, const std::string& name) {
+    std::vector<int> dims;
+    std::vector<double> v = mat_read(file, name, &dims);
+    if ((long)v.size() != size()) throw std::runtime_error("size of " + name + " in " + file + " does not match the grid");
+    for (int i = 0; i < Lx_; i++)
+        for (int j = 0; j < Ly_; j++)
+            for (int k = 0; k < Lz_; k++)
+                data_[((size_t)i * Ly_ + j) * Lz_ + k] = v[((size_t)k * Ly_ + j) * Lx_ + i];
+}
+
+// ---------------------------------------------------------------------------
+// updaters
+// ---------------------------------------------------------------------------
+PropagatorUpdater::PropagatorUpdater(int scheme, const UnitCell& uc, int Lx, int Ly, int Lz, double ds) {
+    check(ps_updater_create(scheme, &uc.c_cell(), Lx, Ly, Lz, ds, &h_));
+}
+
+PropagatorUpdater::PropagatorUpdater(const PropagatorUpdater& rhs) : Updater(rhs) {
+    check(ps_updater_clone(rhs.h_, &h_));
+}
+
+PropagatorUpdater::~PropagatorUpdater() { ps_updater_destroy(h_); }
+
+void PropagatorUpdater::solve(Propagator& q, const Grid& w) { check(ps_updater_solve(h_, w.data(), q.qs(), q.len())); }
+
+void Propagator::set_head(const double* u) { std::memcpy(qs_.data(), u, sizeof(double) * size()); }
+
+double Propagator::Q(int s) const {
+    const double* p = qs_.data() + (size_t)s * size();
+    double acc = 0.0;
+    for (long i = 0; i < size(); i++) acc += p[i];
+    return acc / (double)size();
+}
+
+void DensityUpdater::solve(std::vector<double>& data, const Propagator& q, const Propagator& qc, double cc) const {
+    check(ps_density_solve(rule_, q.qs(), qc.qs(), q.len(), q.size(), q.ds(), cc, data.data()));
+}
+
+void Density::update(const Propagator& q, const Propagator& qc, double cc) {
+    if (up_) {
+        up_->solve(vec(), q, qc, cc);
+    } else {
+        check(ps_density_solve(PS_CONTOUR_TRAPEZOID, q.qs(), qc.qs(), q.len(), q.size(), q.ds(), cc, data()));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Model_AB
+// ---------------------------------------------------------------------------
+Model_AB::Model_AB(const Config& cfg) : Lx_(cfg.Lx()), Ly_(cfg.Ly()), Lz_(cfg.Lz()) {
+    if (cfg.algo_mde_type() == AlgorithmMDEType::ETDRK4)
+        throw std::runtime_error("MDE algorithm ETDRK4 is not provided by the B200 backend (RQM4, OS2)");
+    std::string confine = upper(cfg.get_string("Grid", "confine_geometry", "NONE"));
+    if (!(confine == "NONE" || confine.empty()))
+        throw std::runtime_error("only periodic cells (confine_geometry = None) are provided by the B200 backend");
+    ps_model_ab_params p;
+    std::memset(&p, 0, sizeof(p));
+    p.dim = cfg.dim();
+    p.Lx = Lx_; p.Ly = Ly_; p.Lz = Lz_;
+    p.cell = UnitCell(cfg).c_cell();
+    std::vector<double> Ms = cfg.Ms();
+    if (Ms.size() < 2) throw std::runtime_error("[Algorithm_MDE] Ms needs two entries");
+    p.sA = (int)Ms[0];
+    p.sB = (int)Ms[1];
+    p.chiN = cfg.chiN();
+    std::vector<double> lam = cfg.lam();
+    if (lam.size() < 3) throw std::runtime_error("[Algorithm_SCFT] lam needs three entries");
+    p.lamA = lam[0]; p.lamB = lam[1]; p.lamYita = lam[2];
+    p.mde = cfg.algo_mde_type() == AlgorithmMDEType::OS2 ? PS_MDE_OS2 : PS_MDE_RQM4;
+    p.scft = cfg.algo_scft_type() == AlgorithmSCFTType::ANDERSON ? PS_SCFT_ANDERSON : PS_SCFT_EM;
+    p.n_anderson = cfg.n_Anderson_mixing();
+    p.compressible = cfg.is_compressible() ? 1 : 0;
+    p.contour = cfg.algo_contour_integration_type() == AlgorithmContourType::SIMPSON ? 1 : 0;
+    check(ps_model_ab_create(&p, &h_));
+    // Model_AB::init_field (Model_AB.cc:687-711)
+    const long M = (long)Lx_ * Ly_ * Lz_;
+    std::vector<double> wA(M), wB(M);
+    switch (cfg.get_grid_init_type()) {
+    case GridInitType::FILE_INIT: {
+        Grid a(Lx_, Ly_, Lz_), b(Lx_, Ly_, Lz_);
+        std::string f = cfg.field_data_file();
+        if (!f.empty() && f[0] != '/') f = cfg.dir() + f;
+        a.load_mat(f, "wA");
+        b.load_mat(f, "wB");
+        wA = a.vec();
+        wB = b.vec();
+        break;
+    }
+    case GridInitType::CONSTANT_INIT:
+        std::fill(wA.begin(), wA.end(), 0.5);
+        std::fill(wB.begin(), wB.end(), 0.5);
+        break;
+    default: {
+        // uniform [0, 1) from the seed (the reference's generator is not
+        // reproducible here; Grid.cc:713-725 uses the same range)
+        std::mt19937_64 gen((uint64_t)cfg.seed());
+        std::uniform_real_distribution<double> u(0.0, 1.0);
+        for (long i = 0; i < M; i++) wA[i] = u(gen);
+        for (long i = 0; i < M; i++) wB[i] = u(gen);
+        break;
+    }
+    }
+    set_fields(wA, wB);
+}
+
+Model_AB::~Model_AB() { ps_model_ab_destroy(h_); }
+
+void Model_AB::set_fields(const std::vector<double>& wA, const std::vector<double>& wB) {
+    check(ps_model_ab_set_fields(h_, wA.data(), wB.data()));
+}
+
+void Model_AB::update() { check(ps_model_ab_update(h_, 1)); }
+void Model_AB::update(int n) { check(ps_model_ab_update(h_, n)); }
+
+double Model_AB::H() const {
+    double H, Hw, Hs;
+    check(ps_model_ab_H(h_, &H, &Hw, &Hs));
+    return H;
+}
+double Model_AB::Hw() const {
+    double H, Hw, Hs;
+    check(ps_model_ab_H(h_, &H, &Hw, &Hs));
+    return Hw;
+}
+double Model_AB::Hs() const {
+    double H, Hw, Hs;
+    check(ps_model_ab_H(h_, &H, &Hw, &Hs));
+    return Hs;
+}
+double Model_AB::residual_error() const {
+    double r;
+    check(ps_model_ab_residual(h_, &r));
+    return r;
+}
+double Model_AB::Q() const {
+    double q;
+    check(ps_model_ab_Q(h_, &q));
+    return q;
+}
+
+std::vector<double> Model_AB::field(int which) const {
+    std::vector<double> out((size_t)Lx_ * Ly_ * Lz_);
+    check(ps_model_ab_get(h_, which, out.data()));
+    return out;
+}
+
+// Model_AB::display (Model_AB.cc:383-427), the lines that concern this path
+void Model_AB::display() const {
+    double H, Hw, Hs;
+    check(ps_model_ab_H(h_, &H, &Hw, &Hs));
+    std::cout << std::fixed << std::setprecision(6) << "\tH    = " << H << " = " << Hw << " + " << Hs << "\n";
+    std::cout << std::scientific << std::setprecision(2) << "\tQ_qB = " << Q() << "\n"
+              << "\tResidual Error    = " << residual_error() << "\n";
+    std::cout.unsetf(std::ios::floatfield);
+}
+
+// fields and densities as MAT-file v5 variables (Model_AB::save, :440-469)
+void Model_AB::save(const std::string& file) {
+    std::vector<int> dims = {Lx_, Ly_, Lz_};
+    auto colmajor = [&](const std::vector<double>& v) {
+        std::vector<double> o(v.size());
+        for (int i = 0; i < Lx_; i++)
+            for (int j = 0; j < Ly_; j++)
+                for (int k = 0; k < Lz_; k++)
+                    o[((size_t)k * Ly_ + j) * Lx_ + i] = v[((size_t)i * Ly_ + j) * Lz_ + k];
+        return o;
+    };
+    std::map<std::string, std::pair<std::vector<int>, std::vector<double>>> vars;
+    vars["wA"] = {dims, colmajor(field(PS_FIELD_WA))};
+    vars["wB"] = {dims, colmajor(field(PS_FIELD_WB))};
+    vars["phiA"] = {dims, colmajor(field(PS_FIELD_PHIA))};
+    vars["phiB"] = {dims, colmajor(field(PS_FIELD_PHIB))};
+    mat_write(file, vars);
+}
+
+// ---------------------------------------------------------------------------
+// scft
+// ---------------------------------------------------------------------------
+void scft::run() {
+    if (cfg_.algo_cell_optimization_type() != AlgorithmCellType::SINGLE)
+        std::cout << "note: cell optimisation is not provided by the B200 backend; running a single cell\n";
+    relax();
+}
+
+// scft::relax (src/scft.cc:382-422) with save_data's stop tests
+// (:532-587): non-finite H stops (diverged); residual below thresh_residual
+// after min_iter stops (converged); max_iter stops.  Updates between record
+// points run as one batch of graph replays.
+void scft::relax() {
+    const int max_iter = cfg_.max_iter();
+    const int rec = std::max(1, cfg_.record_interval());
+    const bool save = cfg_.is_save_data();
+    int i = 0;
+    while (i < max_iter) {
+        int n = save ? std::min(rec - (i % rec), max_iter - i) : max_iter - i;
+        static_cast<Model_AB*>(m_)->update(n);
+        i += n;
+        iter_ = i;
+        if (cfg_.is_display() && cfg_.display_interval() > 0 && i % cfg_.display_interval() == 0) {
+            std::cout << i << "\n";
+            m_->display();
+        }
+        if (save && i % rec == 0) {
+            Hlast_ = m_->H();
+            rlast_ = m_->residual_error();
+            if (!std::isfinite(Hlast_)) {
+                std::cout << "\nError: diverge\nIter: " << i << "\nH = " << Hlast_ << "\n";
+                return;
+            }
+            if (i > cfg_.min_iter() && i / rec > 1 && rlast_ < cfg_.thresh_residual()) break;
+        }
+    }
+    Hlast_ = m_->H();
+    rlast_ = m_->residual_error();
+}
+
+}  // namespace polyorder

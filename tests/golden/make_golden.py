@@ -9,6 +9,8 @@ PolyOrder snapshot bundled in the reference):
 
 * 1D/field_in_64.mat, 2D/field_in_32x32.mat: the input fields wA, wB used by
   those example runs (Grid gridInitType = File).
+* {1D,2D}/param.ini: the example config files, copied unchanged to
+  lam1d_param.ini and lam2d_param.ini.
 * {1D,2D}/cell_opt_{rqm4,rqm4_anderson,os2,os2_anderson}.mat: the (a, F)
   pairs written by scft::save_cell (src/scft.cc:589-609) during the Brent
   cell optimisation.  Every entry is a converged SCFT free energy H at cell
@@ -42,7 +44,12 @@ def main(ref_root="/root/reference"):
             key = "%s_%s" % (dim.lower(), tag)
             out[key + "_a"] = np.asarray(d["a"], dtype=np.float64).ravel()
             out[key + "_F"] = np.asarray(d["F"], dtype=np.float64).ravel()
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lam_pins.npz")
+    here = os.path.dirname(os.path.abspath(__file__))
+    # the example config files themselves, unchanged (inputs of the driver test)
+    for dim in ("1D", "2D"):
+        with open(os.path.join(here, "lam%s_param.ini" % dim.lower()), "wb") as f:
+            f.write(z.read(base + "%s/param.ini" % dim))
+    dst = os.path.join(here, "lam_pins.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, sorted(out))
 
