@@ -59,15 +59,24 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Counter + release-flag grid barrier: the last CTA to arrive publishes the
-// barrier index; the others poll the flag with a bounded spin.
+// barrier index; the others poll the flag with a bounded spin.  The CTA
+// barrier before the arrival orders the CTA's writes before thread 0's
+// release (PTX memory model: bar.sync then a release at gpu scope is
+// cumulative); the acquire load and the CTA barrier after it order the
+// CTA's later reads.
 __device__ __forceinline__ bool grid_sync(unsigned* ctr, int* err, unsigned idx) {
     __syncthreads();
     __shared__ int stop;
     if (threadIdx.x == 0) {
         int s = 0;
-        __threadfence();
-        unsigned old = atomicAdd(ctr, 1u);
+        unsigned old = atom_add_acq_rel(ctr, 1u);
         if (old + 1 == idx * gridDim.x) {
             st_release(ctr + 32, idx);
         } else {
@@ -77,7 +86,6 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, int* err, unsigned idx)
                 if (++spins > kSpin) { atomicExch(err, 2); s = 1; break; }
             }
         }
-        __threadfence();
         stop = s;
     }
     __syncthreads();
@@ -354,7 +362,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 double qf = (v[k].x * hf) / Md, qc = (v[k].y * hc) / Md;
                 qf = (4.0 * qf - u.x) / 3.0;
                 qc = (4.0 * qc - u.y) / 3.0;
-                if (role == 0) { of[zi] = qf; oc[zi] = qc; }
+                if (role == 0) of[zi] = qf;
+                if (role == 1 || !next) oc[zi] = qc;
                 double gf = nf[zi], gc = nc[zi];
                 if (role == 0) { gf *= gf; gc *= gc; }
                 v[k] = make_double2(gf * qf, gc * qc);
