@@ -154,6 +154,39 @@ def cpu_baseline(cfg, seconds, threads):
                       "%d OpenMP threads), %.1f s" % (nsteps, threads, dt)}
 
 
+def string_method(ps, iters=10):
+    """Secondary result: the batched string method (40 images, 2D 128x128,
+    Ns 128, 3 SCFT iterations per image per string iteration) against the
+    same SCFT work run image by image through the plain single-model path."""
+    from polystring_b200 import workloads
+    m, shape, L = 40, (128, 128, 1), 8.0
+    Ms = workloads.ms_from(0.35, 128)
+    wa, wb = workloads.string_images(m=m, shape=shape, L=L)
+    cell = ps.make_cell(2, "SQUARE", L)
+    g = ps.StringAB(m, 2, shape, cell, Ms, 18.0, max_iter=3)
+    g.set_images(wa, wb)
+    g.iterate(2)
+    g.synchronize()
+    t0 = time.perf_counter()
+    g.iterate(iters)
+    g.synchronize()
+    tb = (time.perf_counter() - t0) / iters
+    single = ps.ModelAB(2, shape, cell, Ms, 18.0)
+    single.set_fields(wa[0], wb[0])
+    single.update(3)
+    single.synchronize()
+    t0 = time.perf_counter()
+    for s in range(m):
+        single.set_fields(wa[s], wb[s])
+        single.update(3)
+        single.H()
+    ts = time.perf_counter() - t0
+    return {"config": "C3 string, 40 images 128x128, Ms %s, 3 SCFT iterations per image" % list(Ms),
+            "batched_string_iters_per_s": 1.0 / tb, "sequential_plain_gpu_iters_per_s": 1.0 / ts,
+            "speedup_vs_sequential": ts / tb, "launches_per_string_iteration": g.launches_per_iteration(),
+            "timing": "host wall clock around synchronised replays"}
+
+
 def run_reference(args, rank, world):
     """The reference algorithm's CPU restatement on all host threads (rank 0);
     each step is a bounded sample of the same workload."""
@@ -275,6 +308,8 @@ def main():
             "kernel": "propagator sweep (persistent RQM4 kernel), %d launch(es) per iteration" % m.launches_per_propagate(),
             "propagator_share_of_step": prop_s / total_s}
 
+    string = string_method(ps) if rank == 0 and world == 1 else None
+
     cpu = None
     if rank == 0 and world == 1:
         import oracle
@@ -288,7 +323,7 @@ def main():
                 "config": {"workload": WORKLOAD, "grid": list(shape), "Ns": Ns, "Ms": list(cfg["Ms"]),
                            "l2_flush": "inputs > L2 (0.8 GB histories)", "parallelism": "replicas" if world > 1 else "single"},
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clk.summary(), "H_after": H}
+                "clocks": clk.summary(), "H_after": H, "string_method": string}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -163,6 +163,9 @@ AxisPlan make_axis_plan(int Lx, int Ly, int Lz) {
         g.T = (g.S == 1) ? largest_divisor_le(g.nlines, target) : largest_divisor_le(g.S, target);
         g.LP = (g.S == 1 && g.T % 2 == 0) ? g.T + 1 : g.T;
         g.ntiles = g.nlines / g.T;
+        g.tshift = -1;
+        for (int b = 0; b < 12; b++)
+            if ((1 << b) == g.T) g.tshift = b;
         ap.ax[ap.naxes++] = g;
     }
     if (ap.naxes == 0) throw Error(-2, "grid has no axis longer than one point");

@@ -24,6 +24,11 @@ namespace ps {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMaxEPT = 8;   // tiles hold at most 2048 elements (make_axis_plan)
+
+// loop over this thread's tile elements: a fixed, unrolled count with a
+// guard, so that independent global loads are issued back to back
+#define PS_ELEMS(e) _Pragma("unroll") for (int k_ = 0, e = threadIdx.x; k_ < kMaxEPT; k_++, e += kThreads) if (e < nel)
 
 struct TileAddr {
     long base, nstride, lstride;
@@ -48,9 +53,11 @@ struct Elem {
     int sidx;
 };
 
+template <int N>
 __device__ __forceinline__ Elem elem(const LineGeom& g, const TileAddr& a, int e) {
     Elem r;
-    if (g.S == 1) { r.l = e / g.N; r.n = e - r.l * g.N; }
+    if (g.S == 1) { r.l = e / N; r.n = e - r.l * N; }
+    else if (g.tshift >= 0) { r.n = e >> g.tshift; r.l = e & (g.T - 1); }
     else          { r.n = e / g.T; r.l = e - r.n * g.T; }
     r.goff = a.base + (long)r.n * a.nstride + (long)r.l * a.lstride;
     r.sidx = r.n * g.LP + r.l;
@@ -60,8 +67,9 @@ __device__ __forceinline__ Elem elem(const LineGeom& g, const TileAddr& a, int e
 template <int N, int R, int NS, int SIGN>
 __device__ __forceinline__ void run_pass(const double2* in, double2* out, int T, int LP, const double2* tw) {
     const int total = T * (N / R);
+    const int tsh = (T & (T - 1)) == 0 ? __ffs(T) - 1 : -1;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-        int j = b / T;
+        int j = tsh >= 0 ? b >> tsh : b / T;
         int l = b - j * T;
         butterfly<N, R, NS, SIGN>(in, out, LP, l, j, tw);
     }
@@ -109,8 +117,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
 
     if constexpr (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_OUTER) {
         double2* z = p.z[fy] + oz;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             A[el.sidx] = z[el.goff];
         }
         __syncthreads();
@@ -122,8 +130,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         }
         if constexpr (MODE == MODE_OUTER) {
             const double* L = p.L[fy] + oL;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double lv = L[el.goff];
                 double2 v = r[el.sidx];
                 r[el.sidx] = make_double2(v.x * lv, v.y * lv);
@@ -131,8 +139,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             __syncthreads();
             r = tile_fft<N, +1>(r, other(r, A, B), g.T, g.LP, twi);
         }
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             z[el.goff] = r[el.sidx];
         }
     } else if constexpr (MODE == MODE_FIRST_RQM4 || MODE == MODE_FIRST_OS2) {
@@ -142,23 +150,23 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         const double* ec = (fy == 0 ? p.eF[1] : p.eH[1]) + oe;
         const double* qf = p.qin[0] + oq;
         const double* qc = p.qin[1] + oq;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             A[el.sidx] = make_double2(ef[el.goff] * qf[el.goff], ec[el.goff] * qc[el.goff]);
         }
         __syncthreads();
         double2* r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
         double2* z = p.z[fy] + oz;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             z[el.goff] = r[el.sidx];
         }
     } else if constexpr (MODE == MODE_MID_RQM4) {
         if (fy == 0) {
             // full step: u = Re/Im(F^-1 Z1) e^{-w ds/2} / M
             double2* z = p.z[0] + oz;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 A[el.sidx] = z[el.goff];
             }
             __syncthreads();
@@ -167,8 +175,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             const double* ec = p.eF[1] + oe;
             double* uf = p.u[0] + ou;
             double* uc = p.u[1] + ou;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 uf[el.goff] = (v.x * ef[el.goff]) / M;
                 uc[el.goff] = (v.y * ec[el.goff]) / M;
@@ -176,16 +184,16 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         } else {
             // first half step finishes, second half step starts
             double2* z = p.z[1] + oz;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 A[el.sidx] = z[el.goff];
             }
             __syncthreads();
             double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
             const double* hf = p.eH[0] + oe;
             const double* hc = p.eH[1] + oe;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 double a = hf[el.goff], b = hc[el.goff];
                 double qtf = (v.x * a) / M;
@@ -195,15 +203,15 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             __syncthreads();
             double2* r2 = tile_fft<N, -1>(r, other(r, A, B), g.T, g.LP, twf);
             double2* z3 = p.z[2] + oz;
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 z3[el.goff] = r2[el.sidx];
             }
         }
     } else if constexpr (MODE == MODE_END_RQM4 || MODE == MODE_END_OS2) {
         double2* zin = (MODE == MODE_END_RQM4 ? p.z[2] : p.z[0]) + oz;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             A[el.sidx] = zin[el.goff];
         }
         __syncthreads();
@@ -212,8 +220,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         const double* hc = (MODE == MODE_END_RQM4 ? p.eH[1] : p.eF[1]) + oe;
         double* of = p.qout[0] + oq;
         double* oc = p.qout[1] + oq;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             double2 v = r[el.sidx];
             double qf = (v.x * hf[el.goff]) / M;
             double qc = (v.y * hc[el.goff]) / M;
@@ -231,16 +239,16 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
                 const double* nf = (k == 0 ? p.nF[0] : p.nH[0]) + oe;
                 const double* nc = (k == 0 ? p.nF[1] : p.nH[1]) + oe;
                 __syncthreads();
-                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                    Elem el = elem(g, ta, e);
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
                     double2 q = C[el.sidx];
                     A[el.sidx] = make_double2(nf[el.goff] * q.x, nc[el.goff] * q.y);
                 }
                 __syncthreads();
                 double2* r2 = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
                 double2* z = p.z[k] + oz;
-                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                    Elem el = elem(g, ta, e);
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
                     z[el.goff] = r2[el.sidx];
                 }
             }
@@ -249,8 +257,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         // single-axis grids: the whole step inside one tile
         const double* qf = p.qin[0] + oq;
         const double* qc = p.qin[1] + oq;
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             C[el.sidx] = make_double2(qf[el.goff], qc[el.goff]);
         }
         const double* ef = p.eF[0] + oe;
@@ -258,15 +266,15 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         const double* L1 = p.L[0] + oL;
         // sub-step 1: full ds step
         __syncthreads();
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             double2 q = C[el.sidx];
             A[el.sidx] = make_double2(ef[el.goff] * q.x, ec[el.goff] * q.y);
         }
         __syncthreads();
         double2* r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
-        for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-            Elem el = elem(g, ta, e);
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
             double lv = L1[el.goff];
             double2 v = r[el.sidx];
             r[el.sidx] = make_double2(v.x * lv, v.y * lv);
@@ -276,15 +284,15 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         double* of = p.qout[0] + oq;
         double* oc = p.qout[1] + oq;
         if constexpr (MODE == MODE_FULL_OS2) {
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 of[el.goff] = (v.x * ef[el.goff]) / M;
                 oc[el.goff] = (v.y * ec[el.goff]) / M;
             }
         } else {
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 D[el.sidx] = make_double2((v.x * ef[el.goff]) / M, (v.y * ec[el.goff]) / M);
             }
@@ -294,30 +302,30 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             // two ds/2 steps: start from C, keep the intermediate in C
             for (int h = 0; h < 2; h++) {
                 __syncthreads();
-                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                    Elem el = elem(g, ta, e);
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
                     double2 q = C[el.sidx];
                     A[el.sidx] = make_double2(hf[el.goff] * q.x, hc[el.goff] * q.y);
                 }
                 __syncthreads();
                 r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
-                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                    Elem el = elem(g, ta, e);
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
                     double lv = L2[el.goff];
                     double2 v = r[el.sidx];
                     r[el.sidx] = make_double2(v.x * lv, v.y * lv);
                 }
                 __syncthreads();
                 r = tile_fft<N, +1>(r, other(r, A, B), g.T, g.LP, twi);
-                for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                    Elem el = elem(g, ta, e);
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
                     double2 v = r[el.sidx];
                     C[el.sidx] = make_double2((v.x * hf[el.goff]) / M, (v.y * hc[el.goff]) / M);
                 }
             }
             __syncthreads();
-            for (int e = threadIdx.x; e < nel; e += blockDim.x) {
-                Elem el = elem(g, ta, e);
+            PS_ELEMS(e) {
+                Elem el = elem<N>(g, ta, e);
                 double2 q = C[el.sidx];
                 double2 u = D[el.sidx];
                 of[el.goff] = (4.0 * q.x - u.x) / 3.0;

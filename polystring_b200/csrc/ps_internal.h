@@ -49,6 +49,7 @@ struct LineGeom {
     int LP;       // smem line pitch (T or T + 1)
     long nlines;  // lines per field (M / N)
     long ntiles;  // tiles per field (nlines / T)
+    int tshift;   // log2(T) when T is a power of two, else -1
 };
 
 // Pointers used by the fused first / last passes.  A "lane" is one of the
