@@ -157,6 +157,24 @@ int ps_model_ab_H(ps_model_ab* m, double* H, double* Hw, double* Hs);
 int ps_model_ab_residual(ps_model_ab* m, double* res);
 /* qB->Qt() of the last update (src/Model_AB.cc:195) */
 int ps_model_ab_Q(ps_model_ab* m, double* Q);
+/* Forward map at fixed fields: the four propagators, Q and both densities of
+ * Model_AB::update (src/Model_AB.cc:186-199) without the field update.
+ * Afterwards ps_model_ab_Q, ps_model_ab_H and ps_model_ab_get (PHIA, PHIB)
+ * report the map's outputs. */
+int ps_model_ab_forward(ps_model_ab* m);
+/* Reverse mode of that map (RQM4, 2D/3D grids; no counterpart in the
+ * reference, which has no derivatives): with the current fields, writes
+ * dL/dwA and dL/dwB (M doubles each, host memory) for
+ * L = sum_r (dL_dphiA phiA + dL_dphiB phiB) + dL_dQ Q, exact for the
+ * discrete RQM4 chain and contour rule; the forward map is re-evaluated. */
+int ps_model_ab_grad_w(ps_model_ab* m, const double* dL_dphiA, const double* dL_dphiB, double dL_dQ,
+                       double* dL_dwA, double* dL_dwB);
+/* Cell stress d(-ln Q)/dl_i at the current fields for the three cell
+ * lengths l_i of the orthogonal k^2 table (UnitCell.cc:368-418; zero for
+ * unused axes).  At an SCFT saddle point this is dF/dl, the derivative the
+ * reference's Brent cell search (src/scft.cc:589-609) estimates from
+ * converged free energies. */
+int ps_model_ab_stress(ps_model_ab* m, double* dF_dl);
 /* copy one array (PS_FIELD_*) to host memory */
 int ps_model_ab_get(ps_model_ab* m, int which, double* out);
 /* device address of one array (PS_FIELD_*), owned by the context */

@@ -167,6 +167,26 @@ class ModelAB:
         capi.check(lib().ps_model_ab_Q(self._h, ctypes.byref(q)))
         return q.value
 
+    def forward(self):
+        """Evaluate (wA, wB) -> (phiA, phiB, Q) at the current fields, no field update."""
+        capi.check(lib().ps_model_ab_forward(self._h))
+        return self
+
+    def grad_w(self, dL_dphiA, dL_dphiB, dL_dQ=0.0):
+        """Gradient of sum(dL_dphiA*phiA + dL_dphiB*phiB) + dL_dQ*Q with respect
+        to (wA, wB) at the current fields (RQM4, 2D/3D grids)."""
+        a, b = _f64(dL_dphiA), _f64(dL_dphiB)
+        gA, gB = np.zeros(self.shape), np.zeros(self.shape)
+        capi.check(lib().ps_model_ab_grad_w(self._h, capi.dptr(a), capi.dptr(b), float(dL_dQ),
+                                            capi.dptr(gA), capi.dptr(gB)))
+        return gA, gB
+
+    def stress(self):
+        """d(-ln Q)/dl for the three cell lengths at the current fields."""
+        out = np.zeros(3)
+        capi.check(lib().ps_model_ab_stress(self._h, capi.dptr(out)))
+        return out
+
     def get(self, name):
         idx = FIELDS[name]
         if name in ("qA", "qAc"):

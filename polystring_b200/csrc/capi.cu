@@ -225,6 +225,28 @@ int ps_model_ab_Q(ps_model_ab* m, double* Q) {
     });
 }
 
+int ps_model_ab_forward(ps_model_ab* m) {
+    return guarded([&] {
+        if (!m) throw Error(PS_ERR_INVALID, "null handle");
+        m->ctx->forward_only();
+    });
+}
+
+int ps_model_ab_grad_w(ps_model_ab* m, const double* dL_dphiA, const double* dL_dphiB, double dL_dQ,
+                       double* dL_dwA, double* dL_dwB) {
+    return guarded([&] {
+        if (!m || !dL_dphiA || !dL_dphiB || !dL_dwA || !dL_dwB) throw Error(PS_ERR_INVALID, "null argument");
+        m->ctx->grad_w(dL_dphiA, dL_dphiB, dL_dQ, dL_dwA, dL_dwB);
+    });
+}
+
+int ps_model_ab_stress(ps_model_ab* m, double* dF_dl) {
+    return guarded([&] {
+        if (!m || !dF_dl) throw Error(PS_ERR_INVALID, "null argument");
+        m->ctx->stress(dF_dl);
+    });
+}
+
 int ps_model_ab_get(ps_model_ab* m, int which, double* out) {
     return guarded([&] {
         if (!m || !out) throw Error(PS_ERR_INVALID, "null argument");

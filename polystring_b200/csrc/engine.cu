@@ -500,6 +500,7 @@ void ModelAB::set_fields(const double* wA, const double* wB, bool dev) {
     PS_CUDA(cudaStreamSynchronize(st_));
     iter_ = 0;
     fields_set_ = true;
+    forward_done_ = false;
 }
 
 void ModelAB::enqueue_propagate() {
@@ -633,7 +634,7 @@ void ModelAB::propagate(int n) {
 void ModelAB::sync() { PS_CUDA(cudaStreamSynchronize(st_)); }
 
 double ModelAB::Q() {
-    if (iter_ == 0) throw Error(-6, "no iteration has run");
+    if (iter_ == 0 && !forward_done_) throw Error(-6, "no iteration has run");
     double q = 0;
     PS_CUDA(cudaMemcpyAsync(&q, scal_.p, sizeof(double), cudaMemcpyDeviceToHost, st_));
     PS_CUDA(cudaStreamSynchronize(st_));
@@ -641,7 +642,7 @@ double ModelAB::Q() {
 }
 
 void ModelAB::H(double* H, double* Hw, double* Hs) {
-    if (iter_ == 0) throw Error(-6, "no iteration has run");
+    if (iter_ == 0 && !forward_done_) throw Error(-6, "no iteration has run");
     launch_Hw(phiA_.p, phiB_.p, wA_.p, wB_.p, M_, p_.chiN, p_.lamYita, p_.compressible, partial_.p, scal_.p + 1, st_);
     double h[2];
     PS_CUDA(cudaMemcpyAsync(h, scal_.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st_));

@@ -57,6 +57,30 @@ struct LaneFactors {
     const double* H(int t) const { return t < switch_t ? eH[0] : eH[1]; }
 };
 
+// One reverse sweep through a chain of Ns RQM4 steps (adjoint.cu).  Step t
+// maps slice t to slice t + 1 of the history hq and runs in block blk[t]
+// (0 = A, 1 = B).  lambda[Ns] = cst_Ns + (wd[0][Ns] pbarA + wd[1][Ns] pbarB)
+// ho[0]; lambda[t] = A_t' lambda[t+1] + (wd[0][t] pbarA + wd[1][t] pbarB)
+// ho[Ns - t].  The w-gradient of every step accumulates into grad[blk[t]].
+struct AdjointSweep {
+    int Ns;
+    const double* hq;          // (Ns + 1) x M history of the chain
+    const double* ho;          // (Ns + 1) x M history of the partner chain
+    double* lam[2];            // two M buffers (ping-pong); lambda[0] ends in one
+    const double* eF[2];       // e^{-w ds/2} of block A / B
+    const double* eH[2];       // e^{-w ds/4}
+    double* grad[2];           // accumulated w-gradient of block A / B
+    double ds[2];
+    const double* pbarA;       // direct terms (nullable: none)
+    const double* pbarB;
+    const int* blk;            // Ns entries
+    const double* wd[2];       // Ns + 1 weights each
+    double cst_Ns;
+    double2* spec;             // 3 M spectra for the stress (nullable)
+    double* stress_partial;    // Ns x 148 x 3
+    double cl[3];              // 8 pi^2 / l^3 per axis (times the step's ds)
+};
+
 // Work space and pass sequence for two real chains advanced together in one
 // packed complex field.  Histories hold (nsteps + 1) slices of M doubles.
 class PairChain {
@@ -71,6 +95,9 @@ public:
     void enqueue(double* hf, double* hc, long hist_bstride, int nsteps, const LaneFactors& lf,
                  const LaneFactors& lc, long fac_bstride, cudaStream_t st, const double* c_in_fixed = nullptr,
                  double* c_out_fixed = nullptr);
+    // reverse sweep of one chain for the w-gradient and the cell stress (RQM4, 2D/3D)
+    void enqueue_adjoint(const AdjointSweep& s, cudaStream_t st);
+    void prepare_adjoint();
     // kernel launches per pair step
     int launches_per_step() const;
     long M() const { return M_; }
@@ -80,7 +107,7 @@ private:
     int Lx_, Ly_, Lz_, scheme_, nbatch_;
     long M_;
     AxisPlan plan_;
-    DevBuf z_[3], u_[2], L1_, L2_;
+    DevBuf z_[3], u_[2], L1_, L2_, half_;
     bool batched_tables_ = false;
 };
 
@@ -119,12 +146,21 @@ public:
     long iterations() const { return iter_; }
     int status();
     bool persistent_sweep() const { return use_sweep_; }
+    // Adjoint of the forward map (wA, wB) -> (phiA, phiB, Q) at fixed fields:
+    // forward_only() evaluates the map; grad_w() returns the gradient (per
+    // point of M) of sum(phiA_bar phiA + phiB_bar phiB) + Q_bar Q with respect
+    // to wA, wB; stress() returns d(-ln Q)/dl for the three cell lengths
+    void forward_only();
+    void grad_w(const double* phiA_bar, const double* phiB_bar, double Q_bar, double* gA, double* gB);
+    void stress(double* dFdl);
 
 private:
     void enqueue_propagate();
     void enqueue_post();
     void ensure_graphs();
     void init_anderson(const double* wA, const double* wB, bool device_ptrs);
+    void adjoint_weights(std::vector<double>& wAf, std::vector<double>& wBf) const;
+    void ensure_adjoint_buffers(bool spec);
     ModelABParams p_;
     long M_;
     int LA_, LB_, Ns_;
@@ -145,8 +181,10 @@ private:
     // Anderson
     DevBuf hwA_, hdA_, hwB_, hdB_, BA_, BB_;
     AXState* axs_ = nullptr;
+    DevBuf lam_, gA_, gB_, pbA_, pbB_, spec_, stress_part_;
     long iter_ = 0;
     bool fields_set_ = false;
+    bool forward_done_ = false;   // Q, phi of the current fields are valid (forward_only)
     int launches_per_iter_ = 0;
     int launches_per_prop_ = 0;
 };

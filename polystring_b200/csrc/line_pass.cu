@@ -129,6 +129,13 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             r = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
         }
         if constexpr (MODE == MODE_OUTER) {
+            if (p.spec[fy]) {
+                double2* sp = p.spec[fy] + oz;
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
+                    sp[el.goff] = r[el.sidx];
+                }
+            }
             const double* L = p.L[fy] + oL;
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
@@ -192,12 +199,18 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
             const double* hf = p.eH[0] + oe;
             const double* hc = p.eH[1] + oe;
+            double* sf = p.half[0];
+            double* sc = p.half[1];
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 double a = hf[el.goff], b = hc[el.goff];
                 double qtf = (v.x * a) / M;
                 double qtc = (v.y * b) / M;
+                if (sf) {
+                    sf[ou + el.goff] = qtf;
+                    sc[ou + el.goff] = qtc;
+                }
                 r[el.sidx] = make_double2(a * qtf, b * qtc);
             }
             __syncthreads();
@@ -206,6 +219,58 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 z3[el.goff] = r2[el.sidx];
+            }
+        }
+    } else if constexpr (MODE == MODE_END_ADJ) {
+        // lane f: q_t (forward slice), lane c: lambda_{t+1}.  qt2 = S'S'q,
+        // vv = S'S'lambda; lambda_t = (4 vv - S lambda)/3 + direct term; the
+        // step's w-gradient -(ds/3)[lam qt2 + 2 u v + q vv] + (ds/6)[lam Sq + q Slam]
+        double2* zin = p.z[2] + oz;
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
+            A[el.sidx] = zin[el.goff];
+        }
+        __syncthreads();
+        double2* r = tile_fft<N, +1>(A, B, g.T, g.LP, twi);
+        const double* hf = p.eH[0] + oe;
+        const double* hc = p.eH[1] + oe;
+        const double* qv = p.qin[0] + oq;
+        const double* lv = p.qin[1];
+        double* lout = p.qout[1];
+        const double ds = p.gds;
+        PS_ELEMS(e) {
+            Elem el = elem<N>(g, ta, e);
+            const long i = el.goff;
+            double2 v = r[el.sidx];
+            double qt2 = (v.x * hf[i]) / M;
+            double vv = (v.y * hc[i]) / M;
+            double sq = p.u[0][ou + i], sl = p.u[1][ou + i];
+            double uh = p.half[0][ou + i], vh = p.half[1][ou + i];
+            double q = qv[i], lam = lv[i];
+            double lt = (4.0 * vv - sl) / 3.0;
+            if (p.pbarA) lt += (p.wdA * p.pbarA[i] + p.wdB * p.pbarB[i]) * p.other[i];
+            lout[i] = lt;
+            if (p.grad)
+                p.grad[i] += -(ds / 3.0) * (lam * qt2 + 2.0 * uh * vh + q * vv) + (ds / 6.0) * (lam * sq + q * sl);
+            C[el.sidx] = make_double2(0.0, lt);
+        }
+        if (p.chain_next) {
+            for (int k = 0; k < 2; k++) {
+                const double* nf = (k == 0 ? p.nF[0] : p.nH[0]) + oe;
+                const double* nc = (k == 0 ? p.nF[1] : p.nH[1]) + oe;
+                __syncthreads();
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
+                    double2 qq = C[el.sidx];
+                    A[el.sidx] = make_double2(nf[el.goff] * p.next_qf[el.goff], nc[el.goff] * qq.y);
+                }
+                __syncthreads();
+                double2* r2 = tile_fft<N, -1>(A, B, g.T, g.LP, twf);
+                double2* z = p.z[k] + oz;
+                PS_ELEMS(e) {
+                    Elem el = elem<N>(g, ta, e);
+                    z[el.goff] = r2[el.sidx];
+                }
             }
         }
     } else if constexpr (MODE == MODE_END_RQM4 || MODE == MODE_END_OS2) {
@@ -339,7 +404,7 @@ constexpr int kMaxSmem = 200 * 1024;
 
 int buffers_for_mode(int mode) {
     switch (mode) {
-    case MODE_END_RQM4: case MODE_END_OS2: case MODE_FULL_OS2: return 3;
+    case MODE_END_RQM4: case MODE_END_OS2: case MODE_FULL_OS2: case MODE_END_ADJ: return 3;
     case MODE_FULL_RQM4: return 4;
     default: return 2;
     }
@@ -382,6 +447,7 @@ void launch_n(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaSt
     case MODE_END_OS2: launch_nm<N, MODE_END_OS2>(g, p, nbatch, st, po); break;
     case MODE_FULL_RQM4: launch_nm<N, MODE_FULL_RQM4>(g, p, nbatch, st, po); break;
     case MODE_FULL_OS2: launch_nm<N, MODE_FULL_OS2>(g, p, nbatch, st, po); break;
+    case MODE_END_ADJ: launch_nm<N, MODE_END_ADJ>(g, p, nbatch, st, po); break;
     default: throw Error(-1, "unknown line pass mode");
     }
 }

@@ -39,6 +39,7 @@ enum PassMode {
     MODE_END_OS2 = 7,    // inverse Z -> q (+ next step's FIRST)
     MODE_FULL_RQM4 = 8,  // whole RQM4 step when the grid has a single axis
     MODE_FULL_OS2 = 9,   // whole OS2 step when the grid has a single axis
+    MODE_END_ADJ = 10,   // adjoint RQM4 step end: lambda_t, w-gradient, next step's FIRST
 };
 
 // Geometry of one line pass over a (batch of) field(s) of M points.
@@ -73,6 +74,16 @@ struct StepPtrs {
     long bstride_u;          // u scratch buffers
     long bstride_e;          // factor arrays
     long bstride_L;          // k tables
+    // adjoint sweeps (lane f = forward slice q_t, lane c = adjoint lambda_{t+1})
+    double* half[2];         // MID: save S'q and S'lambda (first half-step results)
+    double2* spec[3];        // OUTER: save the spectrum after the forward FFT (field index)
+    double* grad;            // END_ADJ: w-gradient of the step's block, accumulated
+    double gds;              // END_ADJ: ds of the step's block
+    const double* pbarA;     // END_ADJ: direct term (wdA pbarA + wdB pbarB) * other
+    const double* pbarB;
+    const double* other;
+    double wdA, wdB;
+    const double* next_qf;   // END_ADJ chaining: lane f input of the next step
 };
 
 void launch_line_pass(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st);
