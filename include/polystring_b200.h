@@ -113,6 +113,20 @@ int ps_density_solve(int rule, const double* q, const double* qc, int len, long 
                      double* phi);
 int ps_density_solve_device(int rule, const double* q, const double* qc, int len, long long M, double ds,
                             double cc, double* phi, void* stream);
+/* No counterpart in the reference.  ps_density_solve_device for callers that
+ * cannot allocate device memory (a host program that owns all device memory
+ * through its own pool, or a loop that cannot afford the synchronisation of
+ * cudaMalloc / cudaFree): same arguments and result, but the contour-weight
+ * table lives in a fixed device array compiled into the library, so nothing
+ * is allocated.  len (contour points) may not exceed
+ * PS_DENSITY_NOALLOC_MAX_LEN; larger values return PS_ERR_INVALID.  The first
+ * call on a device looks up the table's device address on the current device;
+ * make that first call before any stream capture.  Asynchronous on `stream`.
+ * All calls share one table per device: calls whose kernels may overlap on
+ * the GPU (different streams with no ordering) race on it. */
+#define PS_DENSITY_NOALLOC_MAX_LEN 8192
+int ps_density_solve_device_noalloc(int rule, const double* q, const double* qc, int len, long long M, double ds,
+                                    double cc, double* phi, void* stream);
 
 /* Grid::quadrature on a regular grid: the mean (src/Grid.cc:329-374); with
  * a propagator slice this is Propagator::Q(s) (src/Propagator.cc:85-89). */

@@ -17,6 +17,8 @@ PS_ERR_UNSUPPORTED = -2
 PS_ERR_CUDA = -3
 PS_ERR_QUADRATURE = -4
 PS_ERR_STATE = -6
+# contour points the fixed table of ps_density_solve_device_noalloc holds
+PS_DENSITY_NOALLOC_MAX_LEN = 8192
 
 MDE = {"RQM4": 0, "OS4": 0, "OS2": 1, "PSEUDOSPECTRAL": 1}
 SCFT = {"EM": 0, "ANDERSON": 1}
@@ -60,6 +62,8 @@ SIGNATURES = [
                                         ctypes.c_double, ctypes.c_double, _dp]),
     ("ps_density_solve_device", ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_longlong,
                                                ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    ("ps_density_solve_device_noalloc", ctypes.c_int, [ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_longlong,
+                                                       ctypes.c_double, ctypes.c_double, _vp, _vp]),
     ("ps_grid_mean_device", ctypes.c_int, [_vp, ctypes.c_longlong, _dp, _vp]),
     ("ps_model_ab_create", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.POINTER(_vp)]),
     ("ps_model_ab_destroy", None, [_vp]),
