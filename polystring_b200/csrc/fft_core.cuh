@@ -37,6 +37,15 @@ template <int SIGN> PS_HD double2 mul_si(double2 a) {
     return SIGN < 0 ? mk(a.y, -a.x) : mk(-a.y, a.x);
 }
 
+// x / d rounded to nearest, from r = RN(1/d): q = RN(x r) is within an ulp
+// of x/d, the remainder x - d q is exact in one fma, and one correction step
+// RN(q + (x - d q) r) is the correctly rounded quotient (P. Markstein, IBM
+// J. Res. Dev. 34(1), 1990).  Three FP64 operations instead of a division.
+PS_HD double div_rn(double x, double d, double r) {
+    const double q = x * r;
+    return fma(fma(-d, q, x), r, q);
+}
+
 // sqrt(1/2) and sin(2 pi/3) rounded to double
 #define PS_SQRT1_2 0.70710678118654752440
 #define PS_SIN60 0.86602540378443864676

@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
     const TileAddr ta = tile_addr(g, tile);
     const int nel = N * g.T;
     const double M = p.M;
+    const double rM = 1.0 / M;
 
     const long oz = bz * p.bstride_z, oq = bz * p.bstride_q, oe = bz * p.bstride_e, oL = bz * p.bstride_L;
     const long ou = bz * p.bstride_u;
@@ -185,8 +186,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                uf[el.goff] = (v.x * ef[el.goff]) / M;
-                uc[el.goff] = (v.y * ec[el.goff]) / M;
+                uf[el.goff] = div_rn(v.x * ef[el.goff], M, rM);
+                uc[el.goff] = div_rn(v.y * ec[el.goff], M, rM);
             }
         } else {
             // first half step finishes, second half step starts
@@ -205,8 +206,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 double a = hf[el.goff], b = hc[el.goff];
-                double qtf = (v.x * a) / M;
-                double qtc = (v.y * b) / M;
+                double qtf = div_rn(v.x * a, M, rM);
+                double qtc = div_rn(v.y * b, M, rM);
                 if (sf) {
                     sf[ou + el.goff] = qtf;
                     sc[ou + el.goff] = qtc;
@@ -242,12 +243,12 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             Elem el = elem<N>(g, ta, e);
             const long i = el.goff;
             double2 v = r[el.sidx];
-            double qt2 = (v.x * hf[i]) / M;
-            double vv = (v.y * hc[i]) / M;
+            double qt2 = div_rn(v.x * hf[i], M, rM);
+            double vv = div_rn(v.y * hc[i], M, rM);
             double sq = p.u[0][ou + i], sl = p.u[1][ou + i];
             double uh = p.half[0][ou + i], vh = p.half[1][ou + i];
             double q = qv[i], lam = lv[i];
-            double lt = (4.0 * vv - sl) / 3.0;
+            double lt = div_rn(4.0 * vv - sl, 3.0, 1.0 / 3.0);
             if (p.pbarA) lt += (p.wdA * p.pbarA[i] + p.wdB * p.pbarB[i]) * p.other[i];
             lout[i] = lt;
             if (p.grad)
@@ -288,11 +289,11 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
         PS_ELEMS(e) {
             Elem el = elem<N>(g, ta, e);
             double2 v = r[el.sidx];
-            double qf = (v.x * hf[el.goff]) / M;
-            double qc = (v.y * hc[el.goff]) / M;
+            double qf = div_rn(v.x * hf[el.goff], M, rM);
+            double qc = div_rn(v.y * hc[el.goff], M, rM);
             if constexpr (MODE == MODE_END_RQM4) {
-                qf = (4.0 * qf - p.u[0][ou + el.goff]) / 3.0;
-                qc = (4.0 * qc - p.u[1][ou + el.goff]) / 3.0;
+                qf = div_rn(4.0 * qf - p.u[0][ou + el.goff], 3.0, 1.0 / 3.0);
+                qc = div_rn(4.0 * qc - p.u[1][ou + el.goff], 3.0, 1.0 / 3.0);
             }
             of[el.goff] = qf;
             oc[el.goff] = qc;
@@ -352,14 +353,14 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                of[el.goff] = (v.x * ef[el.goff]) / M;
-                oc[el.goff] = (v.y * ec[el.goff]) / M;
+                of[el.goff] = div_rn(v.x * ef[el.goff], M, rM);
+                oc[el.goff] = div_rn(v.y * ec[el.goff], M, rM);
             }
         } else {
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                D[el.sidx] = make_double2((v.x * ef[el.goff]) / M, (v.y * ec[el.goff]) / M);
+                D[el.sidx] = make_double2(div_rn(v.x * ef[el.goff], M, rM), div_rn(v.y * ec[el.goff], M, rM));
             }
             const double* hf = p.eH[0] + oe;
             const double* hc = p.eH[1] + oe;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
                 PS_ELEMS(e) {
                     Elem el = elem<N>(g, ta, e);
                     double2 v = r[el.sidx];
-                    C[el.sidx] = make_double2((v.x * hf[el.goff]) / M, (v.y * hc[el.goff]) / M);
+                    C[el.sidx] = make_double2(div_rn(v.x * hf[el.goff], M, rM), div_rn(v.y * hc[el.goff], M, rM));
                 }
             }
             __syncthreads();
@@ -393,8 +394,8 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
                 Elem el = elem<N>(g, ta, e);
                 double2 q = C[el.sidx];
                 double2 u = D[el.sidx];
-                of[el.goff] = (4.0 * q.x - u.x) / 3.0;
-                oc[el.goff] = (4.0 * q.y - u.y) / 3.0;
+                of[el.goff] = div_rn(4.0 * q.x - u.x, 3.0, 1.0 / 3.0);
+                oc[el.goff] = div_rn(4.0 * q.y - u.y, 3.0, 1.0 / 3.0);
             }
         }
     }

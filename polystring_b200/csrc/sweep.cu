@@ -186,6 +186,7 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
 
     const long M = G::M;
     const double Md = (double)M;
+    const double rMd = 1.0 / Md;
     const int nb = gridDim.x;
     const long boff = (long)blockIdx.y * a.bstride_batch;   // batch offset of per-problem arrays
     unsigned bar_target = 0;
@@ -321,8 +322,8 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                             if (G::PT % kNT == 0 || p < G::PT) {
                                 long g = s0 + p;
                                 double2 v = buf[pidx<G, LZ>(p)];
-                                uf[g] = (v.x * ef[g]) / Md;
-                                uc[g] = (v.y * ec[g]) / Md;
+                                uf[g] = div_rn(v.x * ef[g], Md, rMd);
+                                uc[g] = div_rn(v.y * ec[g], Md, rMd);
                             }
                         }
                         __syncthreads();
@@ -337,8 +338,8 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                                 int si = pidx<G, LZ>(p);
                                 double2 v = buf[si];
                                 double ha = hfp[g], hb = hcp[g];
-                                double qtf = (v.x * ha) / Md;
-                                double qtc = (v.y * hb) / Md;
+                                double qtf = div_rn(v.x * ha, Md, rMd);
+                                double qtc = div_rn(v.y * hb, Md, rMd);
                                 buf[si] = make_double2(ha * qtf, hb * qtc);
                             }
                         }
@@ -374,10 +375,10 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                     long g = s0 + p;
                     int si = pidx<G, LZ>(p);
                     double2 v = buf[si];
-                    double qf = (v.x * hfp[g]) / Md;
-                    double qc = (v.y * hcp[g]) / Md;
-                    qf = (4.0 * qf - uf[g]) / 3.0;
-                    qc = (4.0 * qc - uc[g]) / 3.0;
+                    double qf = div_rn(v.x * hfp[g], Md, rMd);
+                    double qc = div_rn(v.y * hcp[g], Md, rMd);
+                    qf = div_rn(4.0 * qf - uf[g], 3.0, 1.0 / 3.0);
+                    qc = div_rn(4.0 * qc - uc[g], 3.0, 1.0 / 3.0);
                     if (role == 0) { of[g] = qf; oc[g] = qc; }
                     if (next) buf[si] = make_double2(nf[g] * qf, nc[g] * qc);
                 }

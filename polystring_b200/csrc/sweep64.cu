@@ -55,36 +55,28 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void red_add_release(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
-    unsigned old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// Counter + release-flag grid barrier: the last CTA to arrive publishes the
-// barrier index; the others poll the flag with a bounded spin.  The CTA
-// barrier before the arrival orders the CTA's writes before thread 0's
-// release (PTX memory model: bar.sync then a release at gpu scope is
-// cumulative); the acquire load and the CTA barrier after it order the
-// CTA's later reads.
+// Counter grid barrier: every CTA adds one with release semantics and polls
+// the counter (acquire) until all CTAs of barrier `idx` have arrived, with a
+// bounded spin.  The counter is zeroed before each launch.  The CTA barrier
+// before the arrival orders the CTA's writes before thread 0's release (PTX
+// memory model: bar.sync then a release at gpu scope is cumulative); the
+// acquire load and the CTA barrier after it order the CTA's later reads.
+// Compared with a last-arriver flag, the arrival needs no round trip.
 __device__ __forceinline__ bool grid_sync(unsigned* ctr, int* err, unsigned idx) {
     __syncthreads();
     __shared__ int stop;
     if (threadIdx.x == 0) {
         int s = 0;
-        unsigned old = atom_add_acq_rel(ctr, 1u);
-        if (old + 1 == idx * gridDim.x) {
-            st_release(ctr + 32, idx);
-        } else {
-            long long spins = 0;
-            while (ld_acquire(ctr + 32) < idx) {
-                if (*((volatile int*)err)) { s = 1; break; }
-                if (++spins > kSpin) { atomicExch(err, 2); s = 1; break; }
-            }
+        red_add_release(ctr, 1u);
+        const unsigned target = idx * gridDim.x;
+        long long spins = 0;
+        while (ld_acquire(ctr) < target) {
+            if ((spins & 63) == 63 && *((volatile int*)err)) { s = 1; break; }
+            if (++spins > kSpin) { atomicExch(err, 2); s = 1; break; }
         }
         stop = s;
     }
@@ -253,6 +245,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     const int slab = b & 63, role = b >> 6;
     const long soff = (long)slab * P64;
     const double Md = (double)M64;
+    const double rMd = 1.0 / Md;
     unsigned* ctr = a.bar;
     unsigned bidx = 0;
     unsigned mphase = 0;
@@ -316,14 +309,14 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 for (int k = 0; k < 8; k++) {
                     const int zi = zb + 8 * k;
                     double hf = ef[zi], hc = ec[zi];
-                    ug[soff + zi] = make_double2((v[k].x * (hf * hf)) / Md, (v[k].y * (hc * hc)) / Md);
+                    ug[soff + zi] = make_double2(div_rn(v[k].x * (hf * hf), Md, rMd), div_rn(v[k].y * (hc * hc), Md, rMd));
                 }
             } else {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const int zi = zb + 8 * k;
                     double hf = ef[zi], hc = ec[zi];
-                    double qf = (v[k].x * hf) / Md, qc = (v[k].y * hc) / Md;
+                    double qf = div_rn(v[k].x * hf, Md, rMd), qc = div_rn(v[k].y * hc, Md, rMd);
                     v[k] = make_double2(hf * qf, hc * qc);
                 }
                 plane_forward(v, s, Z3 + soff);
@@ -359,9 +352,9 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 const int zi = zb + 8 * k;
                 double hf = ef[zi], hc = ec[zi];
                 double2 u = s.u[zi];
-                double qf = (v[k].x * hf) / Md, qc = (v[k].y * hc) / Md;
-                qf = (4.0 * qf - u.x) / 3.0;
-                qc = (4.0 * qc - u.y) / 3.0;
+                double qf = div_rn(v[k].x * hf, Md, rMd), qc = div_rn(v[k].y * hc, Md, rMd);
+                qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
+                qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
                 if (role == 0) of[zi] = qf;
                 if (role == 1 || !next) oc[zi] = qc;
                 double gf = nf[zi], gc = nc[zi];

@@ -54,8 +54,27 @@ static double run() {
     return err / mx;
 }
 
+// div_rn against IEEE division for the divisors the kernels use (3 and the
+// point counts of supported grids), over magnitudes 1e-30 .. 1e30
+static double check_div() {
+    const double ds[] = {3.0, 4096.0, 16384.0, 32768.0, 110592.0, 262144.0, 884736.0, 9216.0, 1536.0, 36864.0};
+    unsigned long long s = 88172645463325252ull;
+    long bad = 0;
+    for (double d : ds) {
+        const double r = 1.0 / d;
+        for (int i = 0; i < 200000; i++) {
+            s ^= s << 13; s ^= s >> 7; s ^= s << 17;
+            double u = (double)(s >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+            double x = u * pow(10.0, (int)(s % 61) - 30);
+            if (ps::div_rn(x, d, r) != x / d) bad++;
+        }
+        printf("div %g %ld\n", d, bad);
+    }
+    return (double)bad;
+}
+
 int main() {
-    double e = 0;
+    double e = check_div();
     e = fmax(e, run<2, -1>());   e = fmax(e, run<4, -1>());   e = fmax(e, run<8, -1>());
     e = fmax(e, run<12, -1>());  e = fmax(e, run<16, -1>());  e = fmax(e, run<24, -1>());
     e = fmax(e, run<32, -1>());  e = fmax(e, run<48, -1>());  e = fmax(e, run<64, -1>());
