@@ -87,6 +87,10 @@ typedef struct ps_updater ps_updater;
 typedef struct ps_model_ab ps_model_ab;
 
 const char* ps_version(void);
+/* Tile schedules the line-pass autotuner chose in this process, one line per
+ * tuned grid / scheme / batch (no counterpart in the reference).  Tuning runs
+ * when a model or string context is created; PS_B200_AUTOTUNE=0 disables it. */
+const char* ps_tuning_log(void);
 const char* ps_last_error(void);
 
 /* ---- propagator updaters (the Updater interface, include/Updater.h:44-69) */

@@ -51,6 +51,7 @@ class ModelABParamsC(ctypes.Structure):
 
 SIGNATURES = [
     ("ps_version", ctypes.c_char_p, []),
+    ("ps_tuning_log", ctypes.c_char_p, []),
     ("ps_last_error", ctypes.c_char_p, []),
     ("ps_updater_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(UnitCellC), ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),

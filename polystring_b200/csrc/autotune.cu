@@ -1,0 +1,128 @@
+// autotune.cu -- tile schedules of the line passes chosen by measurement.
+//
+// A line pass stages T lines of one axis in shared memory per CTA.  T sets
+// how many CTAs a pass has, how much shared memory each holds (so how many
+// are resident per SM) and how long the contiguous runs of the strided loads
+// are; which value is fastest depends on the grid, the batch and the scheme.
+// The tile height never changes the arithmetic of a line, so every candidate
+// gives bit-identical results and the choice is purely a timing question.
+//
+// PairChain::autotune times complete contour steps of the chain's own pass
+// sequence (the enqueue() that the propagator graphs capture) on scratch
+// histories with unit fields, over tiles of 512, 1024 and 2048 elements per
+// axis that fit in shared memory, by coordinate descent over the axes (two
+// sweeps), keeping the fastest.  Results are cached per (grid, scheme, batch,
+// table layout) for the life of the process; PS_B200_AUTOTUNE=0 keeps the
+// default 2048-element tiles.
+#include "engine.h"
+#include "field_kernels.h"
+
+#include <cstdio>
+#include <cstdlib>
+#include <array>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+namespace ps {
+
+namespace {
+
+using TuneKey = std::tuple<int, int, int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, std::array<int, 3>> g_tune_cache;   // elements per tile of each axis
+std::string g_tune_log;
+
+bool tuning_enabled() {
+    const char* e = std::getenv("PS_B200_AUTOTUNE");
+    return !(e && e[0] == '0');
+}
+
+}  // namespace
+
+const char* tuning_log() {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    return g_tune_log.c_str();
+}
+
+void PairChain::autotune(cudaStream_t st) {
+    if (plan_.naxes < 2 || !tuning_enabled()) return;
+    const TuneKey key{Lx_, Ly_, Lz_, scheme_, nbatch_, batched_tables_ ? 1 : 0};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            for (int a = 0; a < plan_.naxes; a++) set_tile_elems(plan_.ax[a], it->second[a]);
+            return;
+        }
+    }
+    const int cand[3] = {512, 1024, 2048};
+    const int first_mode = (scheme_ == SCHEME_RQM4) ? MODE_END_RQM4 : MODE_END_OS2;
+    auto fits = [&](int a, int elems) {
+        LineGeom g = plan_.ax[a];
+        set_tile_elems(g, elems);
+        return line_pass_smem_bytes(a == 0 ? first_mode : MODE_OUTER, g) <= kLinePassSmemLimit;
+    };
+
+    // scratch: two histories of nst + 1 slices and unit Boltzmann factors
+    const int nst = 2;
+    const long M = M_;
+    const long hstride = (long)(nst + 1) * M;
+    DevBuf hf((size_t)hstride * nbatch_), hc((size_t)hstride * nbatch_), ef((size_t)M * nbatch_);
+    launch_fill(hf.p, hstride * nbatch_, 1.0, st);
+    launch_fill(hc.p, hstride * nbatch_, 1.0, st);
+    launch_fill(ef.p, M * nbatch_, 1.0, st);
+    LaneFactors lf{{ef.p, ef.p}, {ef.p, ef.p}, nst};
+    cudaEvent_t e0, e1;
+    PS_CUDA(cudaEventCreate(&e0));
+    PS_CUDA(cudaEventCreate(&e1));
+    auto time_plan = [&]() {
+        enqueue(hf.p, hc.p, hstride, nst, lf, lf, M, st);   // warm
+        float best = 1e30f;
+        for (int r = 0; r < 3; r++) {
+            PS_CUDA(cudaEventRecord(e0, st));
+            enqueue(hf.p, hc.p, hstride, nst, lf, lf, M, st);
+            PS_CUDA(cudaEventRecord(e1, st));
+            PS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) best = ms;
+        }
+        return best;
+    };
+
+    std::array<int, 3> choice = {2048, 2048, 2048};
+    for (int a = 0; a < plan_.naxes; a++) set_tile_elems(plan_.ax[a], choice[a]);
+    const float t_default = time_plan();
+    float t_best = t_default;
+    for (int sweep = 0; sweep < 2; sweep++) {
+        for (int a = 0; a < plan_.naxes; a++) {
+            for (int c : cand) {
+                if (c == choice[a] || !fits(a, c)) continue;
+                set_tile_elems(plan_.ax[a], c);
+                const float t = time_plan();
+                if (t < 0.97f * t_best) {
+                    t_best = t;
+                    choice[a] = c;
+                }
+            }
+            set_tile_elems(plan_.ax[a], choice[a]);
+        }
+    }
+    PS_CUDA(cudaEventDestroy(e0));
+    PS_CUDA(cudaEventDestroy(e1));
+    PS_CUDA(cudaStreamSynchronize(st));
+
+    char line[256];
+    std::snprintf(line, sizeof(line), "grid %dx%dx%d %s batch %d: tile elements [%d %d %d] T [%d %d %d], "
+                  "step %.1f us (default %.1f us)\n", Lx_, Ly_, Lz_, scheme_ == SCHEME_RQM4 ? "RQM4" : "OS2",
+                  nbatch_, choice[0], plan_.naxes > 1 ? choice[1] : 0, plan_.naxes > 2 ? choice[2] : 0,
+                  plan_.ax[0].T, plan_.naxes > 1 ? plan_.ax[1].T : 0, plan_.naxes > 2 ? plan_.ax[2].T : 0,
+                  1e3 * t_best / nst, 1e3 * t_default / nst);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = choice;
+    g_tune_log += line;
+}
+
+}  // namespace ps

@@ -59,6 +59,8 @@ extern "C" {
 
 const char* ps_version(void) { return "polystring_b200 0.1 (sm_100a, FP64)"; }
 
+const char* ps_tuning_log(void) { return tuning_log(); }
+
 const char* ps_last_error(void) { return g_last_error.c_str(); }
 
 int ps_updater_create(int scheme, const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds, ps_updater** out) {

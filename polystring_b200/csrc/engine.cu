@@ -144,6 +144,16 @@ static int largest_divisor_le(long n, long cap) {
     return 1;
 }
 
+void set_tile_elems(LineGeom& g, int elems) {
+    const long target = std::max(1, elems / g.N);
+    g.T = (g.S == 1) ? largest_divisor_le(g.nlines, target) : largest_divisor_le(g.S, target);
+    g.LP = (g.S == 1 && g.T % 2 == 0) ? g.T + 1 : g.T;
+    g.ntiles = g.nlines / g.T;
+    g.tshift = -1;
+    for (int b = 0; b < 12; b++)
+        if ((1 << b) == g.T) g.tshift = b;
+}
+
 AxisPlan make_axis_plan(int Lx, int Ly, int Lz) {
     AxisPlan ap;
     const long M = (long)Lx * Ly * Lz;
@@ -159,13 +169,7 @@ AxisPlan make_axis_plan(int Lx, int Ly, int Lz) {
         g.N = N;
         g.S = strides[a];
         g.nlines = M / N;
-        long target = std::max(1, 2048 / N);
-        g.T = (g.S == 1) ? largest_divisor_le(g.nlines, target) : largest_divisor_le(g.S, target);
-        g.LP = (g.S == 1 && g.T % 2 == 0) ? g.T + 1 : g.T;
-        g.ntiles = g.nlines / g.T;
-        g.tshift = -1;
-        for (int b = 0; b < 12; b++)
-            if ((1 << b) == g.T) g.tshift = b;
+        set_tile_elems(g, 2048);
         ap.ax[ap.naxes++] = g;
     }
     if (ap.naxes == 0) throw Error(-2, "grid has no axis longer than one point");
@@ -455,6 +459,7 @@ ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
     launch_fill(hf_.p, M_, 1.0, st_);
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
+    if (!use_sweep_ && !use_sweep64_) chain_->autotune(st_);
     PS_CUDA(cudaStreamSynchronize(st_));
     launches_per_prop_ = (use_sweep_ || use_sweep64_) ? 1 : chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
     launches_per_iter_ = launches_per_prop_ + 2 + 2 + (p.scft == 1 ? 4 : 1);

@@ -44,6 +44,11 @@ struct AxisPlan {
     LineGeom ax[3];
 };
 AxisPlan make_axis_plan(int Lx, int Ly, int Lz);
+// tile of about `elems` elements: T lines, T a divisor of the line count
+// (contiguous axis) or of the stride (outer axes)
+void set_tile_elems(LineGeom& g, int elems);
+// the tile choices of the autotuner so far, one line per tuned chain
+const char* tuning_log();
 
 enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1 };
 
@@ -98,6 +103,8 @@ public:
     // reverse sweep of one chain for the w-gradient and the cell stress (RQM4, 2D/3D)
     void enqueue_adjoint(const AdjointSweep& s, cudaStream_t st);
     void prepare_adjoint();
+    // choose each axis's tile height by timing whole contour steps (after set_tables*)
+    void autotune(cudaStream_t st);
     // kernel launches per pair step
     int launches_per_step() const;
     long M() const { return M_; }

@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
     }
 }
 
-constexpr int kMaxSmem = 200 * 1024;
+constexpr int kMaxSmem = (int)kLinePassSmemLimit;
 
 int buffers_for_mode(int mode) {
     switch (mode) {

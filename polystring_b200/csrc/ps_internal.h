@@ -90,6 +90,7 @@ void launch_line_pass(int mode, const LineGeom& g, const StepPtrs& p, int nbatch
 // sets kernel attributes and builds twiddles; call outside stream capture
 void prepare_line_pass(int mode, const LineGeom& g);
 size_t line_pass_smem_bytes(int mode, const LineGeom& g);
+constexpr size_t kLinePassSmemLimit = 200 * 1024;   // dynamic shared memory of one line-pass CTA
 bool line_size_supported(int N);
 
 // ---------------------------------------------------------------------------

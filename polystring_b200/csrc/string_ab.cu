@@ -196,6 +196,7 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
         }
         chain_->set_tables(L1, L2);
     }
+    chain_->autotune(st_);
     const size_t mM = (size_t)m * M_;
     hf_.alloc((size_t)(Ns_ + 1) * mM);
     hc_.alloc((size_t)(Ns_ + 1) * mM);

@@ -342,7 +342,7 @@ Model_AB::Model_AB(const Config& cfg) : Lx_(cfg.Lx()), Ly_(cfg.Ly()), Lz_(cfg.Lz
     std::string confine = upper(cfg.get_string("Grid", "confine_geometry", "NONE"));
     if (!(confine == "NONE" || confine.empty()))
         throw std::runtime_error("only periodic cells (confine_geometry = None) are provided by the B200 backend");
-    ps_model_ab_params p;
+    ps_model_ab_params& p = p_;
     std::memset(&p, 0, sizeof(p));
     p.dim = cfg.dim();
     p.Lx = Lx_; p.Ly = Ly_; p.Lz = Lz_;
@@ -396,6 +396,31 @@ Model_AB::~Model_AB() { ps_model_ab_destroy(h_); }
 
 void Model_AB::set_fields(const std::vector<double>& wA, const std::vector<double>& wB) {
     check(ps_model_ab_set_fields(h_, wA.data(), wB.data()));
+}
+
+void Model_AB::reset_cell(const Config& cfg) {
+    std::vector<double> wA = field(PS_FIELD_WA), wB = field(PS_FIELD_WB);
+    ps_model_ab* h = nullptr;
+    ps_model_ab_params p = p_;
+    p.cell = UnitCell(cfg).c_cell();
+    check(ps_model_ab_create(&p, &h));
+    ps_model_ab_destroy(h_);
+    h_ = h;
+    p_ = p;
+    set_fields(wA, wB);
+}
+
+std::vector<double> Model_AB::lengths() const {
+    const int d = p_.dim;
+    return {p_.cell.a, d >= 2 ? p_.cell.b : 0.0, d >= 3 ? p_.cell.c : 0.0};
+}
+
+bool Model_AB::has_stress() const { return p_.mde == PS_MDE_RQM4 && p_.dim >= 2; }
+
+std::vector<double> Model_AB::stress() const {
+    std::vector<double> s(3, 0.0);
+    check(ps_model_ab_stress(h_, s.data()));
+    return s;
 }
 
 void Model_AB::update() { check(ps_model_ab_update(h_, 1)); }
@@ -466,9 +491,223 @@ void Model_AB::save(const std::string& file) {
 // scft
 // ---------------------------------------------------------------------------
 void scft::run() {
-    if (cfg_.algo_cell_optimization_type() != AlgorithmCellType::SINGLE)
-        std::cout << "note: cell optimisation is not provided by the B200 backend; running a single cell\n";
+    switch (cfg_.algo_cell_optimization_type()) {
+    case AlgorithmCellType::BRENT:
+        optimize_cell();
+        break;
+    case AlgorithmCellType::MANUAL: {
+        std::vector<double> lo = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_min");
+        std::vector<double> st = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_step");
+        std::vector<double> hi = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_max");
+        lo.resize(3, 0.0); st.resize(3, 1.0); hi.resize(3, 0.0);
+        for (int i = 0; i < 3; i++) if (st[i] <= 0) st[i] = 1.0;
+        for (double a = lo[0]; a <= hi[0] + 1e-12; a += st[0])
+            for (double b = lo[1]; b <= hi[1] + 1e-12; b += st[1])
+                for (double c = lo[2]; c <= hi[2] + 1e-12; c += st[2]) {
+                    cfg_.a(a); cfg_.b(b); cfg_.c(c);
+                    Model_AB* m = static_cast<Model_AB*>(m_);
+                    if (nsolve_ > 0) m->reset_cell(cfg_);
+                    relax();
+                    std::vector<double> l = m->lengths();
+                    trace_.push_back({l[0], l[1], l[2], Hlast_});
+                    nsolve_++;
+                }
+        break;
+    }
+    default:
+        relax();
+    }
+}
+
+void scft::update_cell(double a, double& b, double& c) const {
+    std::vector<double> lo = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_min");
+    lo.resize(3, 0.0);
+    const double a0 = lo[0];
+    b = lo[1];
+    c = lo[2];
+    auto regular = [&](const char* key) {
+        std::string t = upper(cfg_.get_string("Grid", key, "REGULAR"));
+        return t.empty() || t == "REGULAR";
+    };
+    if (cfg_.dim() == 2 && regular("grid_type_y")) b = lo[1] * (a / a0);
+    if (cfg_.dim() == 3 && regular("grid_type_z")) {
+        b = lo[1] * (a / a0);
+        c = lo[2] * (a / a0);
+    }
+}
+
+double scft::solve_cell(double a, double* dFda) {
+    double b, c;
+    update_cell(a, b, c);
+    Model_AB* m = static_cast<Model_AB*>(m_);
+    const bool same = nsolve_ == 0 && a == cfg_.a();
+    cfg_.a(a); cfg_.b(b); cfg_.c(c);
+    if (!same) m->reset_cell(cfg_);
+    const int before = iter_;
     relax();
+    iter_ += before;
+    std::vector<double> l = m->lengths();
+    trace_.push_back({l[0], l[1], l[2], Hlast_});
+    nsolve_++;
+    if (dFda) {
+        // every length scales with a (update_cell), so dF/da = sum_i s_i l_i / a
+        std::vector<double> s = m->stress();
+        *dFda = (s[0] * l[0] + s[1] * l[1] + s[2] * l[2]) / a;
+    }
+    if (cfg_.is_display())
+        std::cout << "cell a = " << a << "  F = " << std::setprecision(12) << Hlast_
+                  << (dFda ? "  dF/da = " + std::to_string(*dFda) : std::string()) << std::setprecision(6) << "\n";
+    return Hlast_;
+}
+
+// BRENT cell optimisation.  The reference brackets the minimum of F(a) from
+// batch_cell_min with steps of batch_cell_step and the golden ratio, then
+// runs Brent's parabolic / golden-section minimiser to the relative
+// tolerance tol_cell (scft.cc:124-309), one converged SCFT solve per trial.
+// Here every solve also yields dF/da from the adjoint stress at the converged
+// fields, so the minimum is found as the root of dF/da: the sign change is
+// bracketed the same way, then Brent-Dekker root finding (inverse quadratic
+// interpolation with bisection safeguards; R. P. Brent, Algorithms for
+// Minimization without Derivatives, 1973, ch. 4) narrows it to tol_cell |a|.
+// Without a stress (1D grids, OS2) the same bracket feeds Brent's
+// derivative-free minimiser (ibid., ch. 5) on F alone.
+void scft::optimize_cell() {
+    std::vector<double> lo = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_min");
+    std::vector<double> st = cfg_.get_list("Algorithm_Cell_Optimization", "batch_cell_step");
+    if (lo.empty() || st.empty()) throw std::runtime_error("BRENT needs batch_cell_min and batch_cell_step");
+    const double tol = cfg_.get_double("Algorithm_Cell_Optimization", "tol_cell", 1e-4);
+    const int max_solves = std::max(4, cfg_.get_integer("Algorithm_Cell_Optimization", "max_iter_cell", 30) + 10);
+    const double GOLD = 1.618034, CGOLD = 0.3819660;
+    Model_AB* m = static_cast<Model_AB*>(m_);
+    const bool grad = m->has_stress();
+    std::map<double, double> Fat;   // F of every solved a
+    auto F_of = [&](double a, double* g) {
+        double F = solve_cell(a, g);
+        Fat[a] = F;
+        return F;
+    };
+    double a0 = lo[0], h = st[0];
+    if (grad) {
+        double g0, g1;
+        F_of(a0, &g0);
+        if (g0 > 0) h = -h;              // F rises to the right: search to the left
+        double a1 = a0 + h;
+        F_of(a1, &g1);
+        while ((g0 < 0) == (g1 < 0) && g1 != 0.0) {
+            if (nsolve_ >= max_solves) throw std::runtime_error("BRENT: no sign change of dF/da was bracketed");
+            a0 = a1; g0 = g1; h *= GOLD;
+            a1 = a0 + h;
+            if (a1 <= 0) throw std::runtime_error("BRENT: the bracket left the positive cell lengths");
+            F_of(a1, &g1);
+        }
+        // Brent-Dekker on g(a) = dF/da over [a0, a1]
+        double xa = a0, fa = g0, xb = a1, fb = g1, xc = xa, fc = fa, d = xb - xa, e = d;
+        while (true) {
+            if ((fb > 0) == (fc > 0)) { xc = xa; fc = fa; d = e = xb - xa; }
+            if (std::fabs(fc) < std::fabs(fb)) { xa = xb; xb = xc; xc = xa; fa = fb; fb = fc; fc = fa; }
+            const double tol1 = 2.0 * 2.2e-16 * std::fabs(xb) + 0.5 * tol * std::fabs(xb);
+            const double xm = 0.5 * (xc - xb);
+            if (std::fabs(xm) <= tol1 || fb == 0.0 || nsolve_ >= max_solves) break;
+            if (std::fabs(e) >= tol1 && std::fabs(fa) > std::fabs(fb)) {
+                double s = fb / fa, p, q;
+                if (xa == xc) {
+                    p = 2.0 * xm * s;
+                    q = 1.0 - s;
+                } else {
+                    double qq = fa / fc, r = fb / fc;
+                    p = s * (2.0 * xm * qq * (qq - r) - (xb - xa) * (r - 1.0));
+                    q = (qq - 1.0) * (r - 1.0) * (s - 1.0);
+                }
+                if (p > 0) q = -q;
+                p = std::fabs(p);
+                if (2.0 * p < std::min(3.0 * xm * q - std::fabs(tol1 * q), std::fabs(e * q))) {
+                    e = d;
+                    d = p / q;
+                } else {
+                    d = xm; e = d;
+                }
+            } else {
+                d = xm; e = d;
+            }
+            xa = xb; fa = fb;
+            xb += std::fabs(d) > tol1 ? d : (xm > 0 ? tol1 : -tol1);
+            F_of(xb, &fb);
+        }
+        amin_ = xb;
+    } else {
+        // bracket a minimum of F by golden steps, then Brent's minimiser
+        double fa0 = F_of(a0, nullptr);
+        double a1 = a0 + h, fa1 = F_of(a1, nullptr);
+        if (fa1 > fa0) { std::swap(a0, a1); std::swap(fa0, fa1); }
+        double a2 = a1 + GOLD * (a1 - a0), fa2 = F_of(a2, nullptr);
+        while (fa1 > fa2) {
+            if (nsolve_ >= max_solves) throw std::runtime_error("BRENT: no minimum of F was bracketed");
+            a0 = a1; fa0 = fa1; a1 = a2; fa1 = fa2;
+            a2 = a1 + GOLD * (a1 - a0);
+            if (a2 <= 0) throw std::runtime_error("BRENT: the bracket left the positive cell lengths");
+            fa2 = F_of(a2, nullptr);
+        }
+        double lo_a = std::min(a0, a2), hi_a = std::max(a0, a2);
+        double x = a1, w = a1, v = a1, fx = fa1, fw = fa1, fv = fa1, d = 0.0, e = 0.0;
+        while (nsolve_ < max_solves) {
+            const double xm = 0.5 * (lo_a + hi_a);
+            const double tol1 = tol * std::fabs(x) + 1e-20, tol2 = 2.0 * tol1;
+            if (std::fabs(x - xm) <= tol2 - 0.5 * (hi_a - lo_a)) break;
+            bool golden = true;
+            if (std::fabs(e) > tol1) {
+                double r = (x - w) * (fx - fv), q = (x - v) * (fx - fw), p = (x - v) * q - (x - w) * r;
+                q = 2.0 * (q - r);
+                if (q > 0) p = -p;
+                q = std::fabs(q);
+                const double eprev = e;
+                e = d;
+                if (std::fabs(p) < std::fabs(0.5 * q * eprev) && p > q * (lo_a - x) && p < q * (hi_a - x)) {
+                    d = p / q;
+                    const double u = x + d;
+                    if (u - lo_a < tol2 || hi_a - u < tol2) d = xm > x ? tol1 : -tol1;
+                    golden = false;
+                }
+            }
+            if (golden) {
+                e = x >= xm ? lo_a - x : hi_a - x;
+                d = CGOLD * e;
+            }
+            const double u = std::fabs(d) >= tol1 ? x + d : x + (d > 0 ? tol1 : -tol1);
+            const double fu = F_of(u, nullptr);
+            if (fu <= fx) {
+                (u >= x ? lo_a : hi_a) = x;
+                v = w; fv = fw; w = x; fw = fx; x = u; fx = fu;
+            } else {
+                (u < x ? lo_a : hi_a) = u;
+                if (fu <= fw || w == x) { v = w; fv = fw; w = u; fw = fu; }
+                else if (fu <= fv || v == x || v == w) { v = u; fv = fu; }
+            }
+        }
+        amin_ = x;
+    }
+    // leave the model at the optimum (the last solve may have been elsewhere)
+    const std::vector<double>& last = trace_.back();
+    double b, c;
+    update_cell(amin_, b, c);
+    if (std::fabs(last[0] - amin_) > 0.0) solve_cell(amin_, nullptr);
+    Fmin_ = Hlast_;
+    std::vector<double> l = m->lengths();
+    std::cout << "amin = " << std::setprecision(10) << l[0] << " bmin = " << l[1] << " cmin = " << l[2] << "\n"
+              << "Fmin = " << std::setprecision(15) << Fmin_ << std::setprecision(6) << "\n";
+}
+
+void scft::save_cell(const std::string& file) const {
+    const int n = (int)trace_.size();
+    std::vector<double> as(n), bs(n), cs(n), Fs(n);
+    for (int i = 0; i < n; i++) {
+        as[i] = trace_[i][0]; bs[i] = trace_[i][1]; cs[i] = trace_[i][2]; Fs[i] = trace_[i][3];
+    }
+    std::map<std::string, std::pair<std::vector<int>, std::vector<double>>> vars;
+    vars["a"] = {{n, 1}, as};
+    vars["b"] = {{n, 1}, bs};
+    vars["c"] = {{n, 1}, cs};
+    vars["F"] = {{n, 1}, Fs};
+    mat_write(file, vars);
 }
 
 // scft::relax (src/scft.cc:382-422) with save_data's stop tests

@@ -17,7 +17,8 @@
 //   Density         include/Density.h:40-88, Simpson (src/Simpson.cc),
 //                   Quad4_Closed (src/Quadrature4.cc)
 //   Model, Model_AB include/Model.h:46-87, include/Model_AB.h:48-114
-//   scft            include/scft.h:56-109 (SINGLE relax loop, record/convergence)
+//   scft            include/scft.h:56-109 (relax loop, record/convergence; SINGLE,
+//                   MANUAL and BRENT cell runs, scft.cc:40-309)
 //
 // Errors from the device are reported by throwing std::runtime_error with
 // the library's message (the reference calls exit(1) on configuration errors).
@@ -252,26 +253,52 @@ public:
     void save(const std::string& file) override;
     std::vector<double> field(int which) const;   // PS_FIELD_*
     void set_fields(const std::vector<double>& wA, const std::vector<double>& wB);
+    // scft::reset_model with DATA_INIT (scft.cc:362-380, Model_AB.cc:20-28):
+    // the same model on the cell of cfg, continuing from the current fields
+    void reset_cell(const Config& cfg);
+    // the cell lengths (lx, ly, lz) the model runs on
+    std::vector<double> lengths() const;
+    // d(-ln Q)/dl_i at the current fields (adjoint of the RQM4 chain; 2D/3D)
+    bool has_stress() const;
+    std::vector<double> stress() const;
 
 private:
     ps_model_ab* h_ = nullptr;
+    ps_model_ab_params p_;
     int Lx_, Ly_, Lz_;
 };
 
 class scft {
 public:
     scft(const Config& cfg, Model* pmodel) : cfg_(cfg), m_(pmodel) {}
-    void run();      // SINGLE cell: relax()
+    // scft::run (src/scft.cc:40-105): SINGLE relaxes the configured cell;
+    // MANUAL relaxes every cell of the batch_cell_min/step/max grid; BRENT
+    // finds the cell length a of least free energy (see optimize_cell)
+    void run();
     void relax();    // scft::relax (src/scft.cc:382-422)
     int iterations() const { return iter_; }
     double final_H() const { return Hlast_; }
     double final_residual() const { return rlast_; }
+    // cells solved so far (lx, ly, lz, F), the as/bs/cs/Fs record of scft.h
+    const std::vector<std::vector<double>>& cell_trace() const { return trace_; }
+    double amin() const { return amin_; }
+    double Fmin() const { return Fmin_; }
+    // the cell record as a MAT-file (scft::save_cell, src/scft.cc:589-609)
+    void save_cell(const std::string& file) const;
 
 private:
-    const Config& cfg_;
+    // scft::update_cell (src/scft.cc:107-121): b and c follow a on regular grids
+    void update_cell(double a, double& b, double& c) const;
+    // relax on cell a (continuing from the current fields); returns F = H and,
+    // when dFda is given, dF/da from the adjoint stress
+    double solve_cell(double a, double* dFda);
+    void optimize_cell();
+    Config cfg_;
     Model* m_;
-    int iter_ = 0;
+    int iter_ = 0, nsolve_ = 0;
     double Hlast_ = 0.0, rlast_ = 0.0;
+    double amin_ = 0.0, Fmin_ = 0.0;
+    std::vector<std::vector<double>> trace_;
 };
 
 }  // namespace polyorder

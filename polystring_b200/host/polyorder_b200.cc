@@ -57,7 +57,10 @@ int main(int argc, char** argv) {
         polyorder::scft sim(cfg, &m);
         sim.run();
         double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (cfg.is_save_data()) m.save(cfg.dir() + cfg.base_dir() + cfg.data_file() + ".mat");
+        if (cfg.is_save_data()) {
+            m.save(cfg.dir() + cfg.base_dir() + cfg.data_file() + ".mat");
+            if (!sim.cell_trace().empty()) sim.save_cell(cfg.dir() + cfg.base_dir() + cfg.data_file() + "_cell.mat");
+        }
         std::printf("iterations = %d\n", sim.iterations());
         std::printf("residual = %.6e\n", sim.final_residual());
         std::printf("H = %.15f\n", sim.final_H());
