@@ -228,6 +228,30 @@ int ps_string_ab_get(ps_string_ab* s, int which, double* out);
 int ps_string_ab_synchronize(ps_string_ab* s);
 int ps_string_ab_launches_per_iteration(ps_string_ab* s);
 
+/* ---- independent solves of uneven grids and Ns, advanced together ------- */
+/* The reference runs independent solves one per host thread
+ * (scft/polystring_AB_backThread.cc).  A batch holds n Model_AB solves,
+ * each with its own parameters p[k] (RQM4; 2D or 3D grids with axis lengths
+ * 16, 24, 32, 48, 64, 96 or 128; Ms, chiN, cell, EM or Anderson may all
+ * differ).  Each line pass of contour step t is one launch over every solve
+ * that has a step t; one batch iteration (= one Model_AB::update of every
+ * solve) is one CUDA graph.  Results equal those of each solve run alone on
+ * the per-pass path. */
+typedef struct ps_batch_ab ps_batch_ab;
+int ps_batch_ab_create(const ps_model_ab_params* p, int n, ps_batch_ab** out);
+void ps_batch_ab_destroy(ps_batch_ab* b);
+int ps_batch_ab_set_fields(ps_batch_ab* b, int k, const double* wA, const double* wB);
+int ps_batch_ab_update(ps_batch_ab* b, int n_iter);
+/* update between CUDA events on the batch stream; device milliseconds */
+int ps_batch_ab_update_timed(ps_batch_ab* b, int n_iter, double* total_ms);
+int ps_batch_ab_H(ps_batch_ab* b, int k, double* H, double* Hw, double* Hs);
+int ps_batch_ab_residual(ps_batch_ab* b, int k, double* res);
+int ps_batch_ab_get(ps_batch_ab* b, int k, int which, double* out);
+int ps_batch_ab_synchronize(ps_batch_ab* b);
+int ps_batch_ab_launches_per_iteration(ps_batch_ab* b);
+/* sum over solves of 2 Ns M: gridpoint contour steps of one batch iteration */
+int ps_batch_ab_gridpoint_steps(ps_batch_ab* b, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,7 +22,7 @@ import numpy as np
 from . import capi
 from .capi import PSError, make_cell, FIELDS, RULES
 
-__all__ = ["RQM4", "PseudoSpectral", "ModelAB", "density", "grid_mean", "make_cell", "PSError", "lib"]
+__all__ = ["RQM4", "PseudoSpectral", "ModelAB", "BatchAB", "density", "grid_mean", "make_cell", "PSError", "lib"]
 
 
 def lib():
@@ -103,6 +103,24 @@ def grid_mean(x_cuda):
     return out.value
 
 
+def _params(dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft="EM", n_anderson=5,
+            compressible=False, contour="Simpson"):
+    """ps_model_ab_params of one Model_AB (the [Model] / [Grid] / [Algorithm_*] values of a config)."""
+    Lx, Ly, Lz = shape
+    p = capi.ModelABParamsC()
+    p.dim, p.Lx, p.Ly, p.Lz = dim, Lx, Ly, Lz
+    p.cell = cell
+    p.sA, p.sB = Ms
+    p.chiN = chiN
+    p.lamA, p.lamB, p.lamYita = lam
+    p.mde = capi.MDE[mde.upper()]
+    p.scft = capi.SCFT[scft.upper()]
+    p.n_anderson = n_anderson
+    p.compressible = 1 if compressible else 0
+    p.contour = capi.CONTOUR[contour.upper()]
+    return p
+
+
 class ModelAB:
     """Model_AB on the device: one SCFT iteration is one replay of a captured
     CUDA graph (propagators, Q, densities, field update)."""
@@ -110,17 +128,7 @@ class ModelAB:
     def __init__(self, dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft="EM",
                  n_anderson=5, compressible=False, contour="Simpson"):
         Lx, Ly, Lz = shape
-        p = capi.ModelABParamsC()
-        p.dim, p.Lx, p.Ly, p.Lz = dim, Lx, Ly, Lz
-        p.cell = cell
-        p.sA, p.sB = Ms
-        p.chiN = chiN
-        p.lamA, p.lamB, p.lamYita = lam
-        p.mde = capi.MDE[mde.upper()]
-        p.scft = capi.SCFT[scft.upper()]
-        p.n_anderson = n_anderson
-        p.compressible = 1 if compressible else 0
-        p.contour = capi.CONTOUR[contour.upper()]
+        p = _params(dim, shape, cell, Ms, chiN, lam, mde, scft, n_anderson, compressible, contour)
         h = ctypes.c_void_p()
         capi.check(lib().ps_model_ab_create(ctypes.byref(p), ctypes.byref(h)))
         self._h = h
@@ -278,4 +286,78 @@ class StringAB:
         h = getattr(self, "_h", None)
         if h:
             lib().ps_string_ab_destroy(h)
+            self._h = None
+
+
+class BatchAB:
+    """Independent Model_AB solves of uneven grids, contour lengths and
+    parameters advanced together (the reference runs such solves one per host
+    thread, scft/polystring_AB_backThread.cc).  `solves` is a list of dicts of
+    ModelAB's constructor arguments (dim, shape, cell, Ms, chiN, lam, scft,
+    n_anderson, compressible, contour; RQM4 only).  update(n) runs n
+    Model_AB::update iterations of every solve; each line pass of a contour
+    step is one launch over all solves still running."""
+
+    def __init__(self, solves):
+        n = len(solves)
+        arr = (capi.ModelABParamsC * n)()
+        self.shapes, self.Ms = [], []
+        for i, sv in enumerate(solves):
+            arr[i] = _params(**sv)
+            self.shapes.append(tuple(sv["shape"]))
+            self.Ms.append(tuple(sv["Ms"]))
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_batch_ab_create(arr, n, ctypes.byref(h)))
+        self._h = h
+        self.n = n
+
+    def set_fields(self, k, wA, wB):
+        wA, wB = _f64(wA), _f64(wB)
+        capi.check(lib().ps_batch_ab_set_fields(self._h, int(k), capi.dptr(wA), capi.dptr(wB)))
+
+    def update(self, n=1):
+        capi.check(lib().ps_batch_ab_update(self._h, int(n)))
+
+    def update_timed(self, n):
+        """update(n) between CUDA events on the batch stream; device ms."""
+        ms = ctypes.c_double()
+        capi.check(lib().ps_batch_ab_update_timed(self._h, int(n), ctypes.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        capi.check(lib().ps_batch_ab_synchronize(self._h))
+
+    def H(self, k):
+        H, Hw, Hs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        capi.check(lib().ps_batch_ab_H(self._h, int(k), ctypes.byref(H), ctypes.byref(Hw), ctypes.byref(Hs)))
+        return H.value, Hw.value, Hs.value
+
+    def residual_error(self, k):
+        r = ctypes.c_double()
+        capi.check(lib().ps_batch_ab_residual(self._h, int(k), ctypes.byref(r)))
+        return r.value
+
+    def get(self, k, name):
+        shape, Ms = self.shapes[k], self.Ms[k]
+        if name in ("qA", "qAc"):
+            out = np.zeros((Ms[0],) + shape)
+        elif name in ("qB", "qBc"):
+            out = np.zeros((Ms[1],) + shape)
+        else:
+            out = np.zeros(shape)
+        capi.check(lib().ps_batch_ab_get(self._h, int(k), FIELDS[name], capi.dptr(out)))
+        return out
+
+    def launches_per_iteration(self):
+        return lib().ps_batch_ab_launches_per_iteration(self._h)
+
+    def gridpoint_steps(self):
+        v = ctypes.c_double()
+        capi.check(lib().ps_batch_ab_gridpoint_steps(self._h, ctypes.byref(v)))
+        return v.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().ps_batch_ab_destroy(h)
             self._h = None

@@ -95,6 +95,17 @@ SIGNATURES = [
     ("ps_string_ab_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("ps_string_ab_synchronize", ctypes.c_int, [_vp]),
     ("ps_string_ab_launches_per_iteration", ctypes.c_int, [_vp]),
+    ("ps_batch_ab_create", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ps_batch_ab_destroy", None, [_vp]),
+    ("ps_batch_ab_set_fields", ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
+    ("ps_batch_ab_update", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("ps_batch_ab_update_timed", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    ("ps_batch_ab_H", ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _dp]),
+    ("ps_batch_ab_residual", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    ("ps_batch_ab_get", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
+    ("ps_batch_ab_synchronize", ctypes.c_int, [_vp]),
+    ("ps_batch_ab_launches_per_iteration", ctypes.c_int, [_vp]),
+    ("ps_batch_ab_gridpoint_steps", ctypes.c_int, [_vp, _dp]),
 ]
 
 _lib = None

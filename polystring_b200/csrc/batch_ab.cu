@@ -1,0 +1,211 @@
+// batch_ab.cu -- many independent Model_AB solves, of uneven grid sizes,
+// contour lengths Ns, block fractions, cells and chiN, advanced together.
+//
+// The reference runs independent solves one per host thread
+// (scft/polystring_AB_backThread.cc); on one B200 a single small solve
+// leaves most SMs idle between launches.  Here every member keeps its own
+// Model_AB state (histories, fields, Anderson ring, per-solve reductions) but
+// its propagator passes run in grouped launches: one launch per line pass of
+// contour step t covers every solve that still has a step t (solves sorted by
+// Ns, so the active ones are a prefix), each CTA running the pass body of its
+// own solve (grouped_pass.cu).  Members are grouped by the number of grid
+// axes longer than one (2 or 3), which fixes the pass sequence of a step.  One
+// batch iteration -- all propagators, then every member's Q, densities and
+// field update -- is captured once as a CUDA graph and replayed.
+#include "batch_ab.h"
+
+#include <algorithm>
+#include <numeric>
+
+namespace ps {
+
+namespace {
+
+// pass kinds of a step: (mode, axis role, second-half-step field)
+const int kPass[9][3] = {{MODE_FIRST_RQM4, GROUP_AX_IN, 0}, {MODE_MID_RQM4, GROUP_AX_IN, 0},
+                         {MODE_END_RQM4, GROUP_AX_IN, 0},   {MODE_FWD, GROUP_AX_MID, 0},
+                         {MODE_FWD, GROUP_AX_MID, 1},       {MODE_INV, GROUP_AX_MID, 0},
+                         {MODE_INV, GROUP_AX_MID, 1},       {MODE_OUTER, GROUP_AX_OUT, 0},
+                         {MODE_OUTER, GROUP_AX_OUT, 1}};
+enum { K_FIRST, K_MID, K_END, K_FWD, K_FWD3, K_INV, K_INV3, K_OUT, K_OUT3 };
+
+}  // namespace
+
+BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
+    if (ps.empty()) throw Error(-1, "a batch needs at least one solve");
+    grouped_prepare();
+    PS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    try {
+        for (const ModelABParams& p : ps) {
+            if (p.mde != 0) throw Error(-2, "batched solves use RQM4");
+            const int sizes[3] = {p.Lx, p.Ly, p.Lz};
+            for (int n : sizes)
+                if (n > 1 && !grouped_size_supported(n))
+                    throw Error(-2, "batched solves support axis lengths 16, 24, 32, 48, 64, 96, 128");
+            m_.push_back(new ModelAB(p, true));
+            if (m_.back()->chain()->plan().naxes < 2) throw Error(-2, "batched solves need 2D or 3D grids");
+        }
+        for (int na = 2; na <= 3; na++) {
+            Group g;
+            g.naxes = na;
+            for (int k = 0; k < (int)m_.size(); k++)
+                if (m_[k]->chain()->plan().naxes == na) g.members.push_back(k);
+            if (g.members.empty()) continue;
+            std::stable_sort(g.members.begin(), g.members.end(),
+                             [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
+            build_group(g);
+            groups_.push_back(std::move(g));
+        }
+    } catch (...) {
+        for (auto* m : m_) delete m;
+        for (auto& g : groups_) {
+            cudaFree(g.dev);
+            for (auto* p : g.prefix_dev) cudaFree(p);
+        }
+        cudaStreamDestroy(st_);
+        throw;
+    }
+}
+
+BatchAB::~BatchAB() {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (auto& g : groups_) {
+        cudaFree(g.dev);
+        for (auto* p : g.prefix_dev) cudaFree(p);
+    }
+    for (auto* m : m_) delete m;
+    if (st_) cudaStreamDestroy(st_);
+}
+
+void BatchAB::build_group(Group& g) {
+    std::vector<GroupSolve> d(g.members.size());
+    for (size_t i = 0; i < g.members.size(); i++) {
+        ModelAB& m = *m_[g.members[i]];
+        PairChain& c = *m.chain();
+        GroupSolve& s = d[i];
+        s.naxes = c.plan().naxes;
+        for (int a = 0; a < s.naxes; a++) {
+            s.ax[a] = c.plan().ax[a];
+            s.tw[a] = twiddle_table(s.ax[a].N);
+        }
+        s.Ns = m.Ns(); s.LA = m.LA(); s.LB = m.LB();
+        s.M = (double)m.M();
+        s.hf = m.hist_f(); s.hc = m.hist_c();
+        for (int i3 = 0; i3 < 3; i3++) s.z[i3] = c.z(i3);
+        s.u[0] = c.u(0); s.u[1] = c.u(1);
+        s.L1 = c.L1(); s.L2 = c.L2();
+        s.eF[0] = m.factor(1, 0); s.eF[1] = m.factor(1, 1);
+        s.eH[0] = m.factor(0, 0); s.eH[1] = m.factor(0, 1);
+        g.Ns.push_back(s.Ns);
+        g.Ns_max = std::max(g.Ns_max, s.Ns);
+    }
+    PS_CUDA(cudaMalloc(&g.dev, sizeof(GroupSolve) * d.size()));
+    PS_CUDA(cudaMemcpy(g.dev, d.data(), sizeof(GroupSolve) * d.size(), cudaMemcpyHostToDevice));
+    for (int k = 0; k < 9; k++) {
+        const int mode = kPass[k][0], ax = kPass[k][1], p3 = kPass[k][2];
+        if (ax == GROUP_AX_MID && g.naxes < 3) continue;
+        std::vector<int>& pre = g.prefix[k];
+        pre.assign(d.size() + 1, 0);
+        for (size_t i = 0; i < d.size(); i++) {
+            pre[i + 1] = pre[i] + grouped_ctas(d[i], mode, ax, p3);
+            const int a = ax == GROUP_AX_IN ? 0 : (ax == GROUP_AX_MID ? 1 : d[i].naxes - 1);
+            g.smem[k] = std::max(g.smem[k], line_pass_smem_bytes(mode, d[i].ax[a]));
+        }
+        if (g.smem[k] > kLinePassSmemLimit) throw Error(-2, "a batched line pass tile does not fit in shared memory");
+        PS_CUDA(cudaMalloc(&g.prefix_dev[k], sizeof(int) * pre.size()));
+        PS_CUDA(cudaMemcpy(g.prefix_dev[k], pre.data(), sizeof(int) * pre.size(), cudaMemcpyHostToDevice));
+    }
+}
+
+void BatchAB::enqueue_iteration() {
+    int launches = 0;
+    int Ns_max = 0;
+    for (auto& g : groups_) Ns_max = std::max(Ns_max, g.Ns_max);
+    for (int t = 0; t < Ns_max; t++) {
+        for (auto& g : groups_) {
+            // members still running at step t: a prefix of the Ns-sorted list
+            int na = 0;
+            while (na < (int)g.Ns.size() && g.Ns[na] > t) na++;
+            if (na == 0) continue;
+            auto pass = [&](int k) {
+                grouped_launch(kPass[k][0], kPass[k][1], kPass[k][2], g.dev, g.prefix_dev[k], na, g.prefix[k][na],
+                               g.smem[k], t, st_);
+                launches++;
+            };
+            const bool three = g.naxes == 3;
+            if (t == 0) pass(K_FIRST);
+            if (three) pass(K_FWD);
+            pass(K_OUT);
+            if (three) pass(K_INV);
+            pass(K_MID);
+            if (three) pass(K_FWD3);
+            pass(K_OUT3);
+            if (three) pass(K_INV3);
+            pass(K_END);
+        }
+    }
+    for (auto* m : m_) {
+        m->enqueue_post(st_);
+        launches += m->launches_per_iteration() - m->launches_per_propagate();
+    }
+    launches_ = launches;
+}
+
+ModelAB& BatchAB::model(int k) {
+    if (k < 0 || k >= (int)m_.size()) throw Error(-1, "solve index out of range");
+    return *m_[k];
+}
+
+void BatchAB::set_fields(int k, const double* wA, const double* wB, bool device_ptrs) {
+    sync();
+    model(k).set_fields(wA, wB, device_ptrs);
+}
+
+void BatchAB::update(int n) {
+    sync();
+    for (auto* m : m_)
+        if (!m->has_fields()) throw Error(-6, "fields of every solve must be set before the batch runs");
+    if (!graph_) {
+        PS_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t g = nullptr;
+        try {
+            enqueue_iteration();
+        } catch (...) {
+            cudaStreamEndCapture(st_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        PS_CUDA(cudaStreamEndCapture(st_, &g));
+        cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) throw Error(-3, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    for (int i = 0; i < n; i++) PS_CUDA(cudaGraphLaunch(graph_, st_));
+    for (auto* m : m_) m->advance(n);
+}
+
+double BatchAB::update_timed(int n) {
+    cudaEvent_t e0, e1;
+    PS_CUDA(cudaEventCreate(&e0));
+    PS_CUDA(cudaEventCreate(&e1));
+    update(0);
+    PS_CUDA(cudaEventRecord(e0, st_));
+    update(n);
+    PS_CUDA(cudaEventRecord(e1, st_));
+    PS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ms;
+}
+
+void BatchAB::sync() { PS_CUDA(cudaStreamSynchronize(st_)); }
+
+double BatchAB::gridpoint_steps_per_iteration() const {
+    double s = 0.0;
+    for (auto* m : m_) s += 2.0 * m->Ns() * (double)m->M();
+    return s;
+}
+
+}  // namespace ps

@@ -1,0 +1,46 @@
+// batch_ab.h -- independent Model_AB solves of uneven grids and contour
+// lengths advanced together (see batch_ab.cu).
+#pragma once
+
+#include <vector>
+
+#include "engine.h"
+#include "grouped_pass.h"
+
+namespace ps {
+
+class BatchAB {
+public:
+    explicit BatchAB(const std::vector<ModelABParams>& ps);
+    ~BatchAB();
+    int size() const { return (int)m_.size(); }
+    ModelAB& model(int k);
+    void set_fields(int k, const double* wA, const double* wB, bool device_ptrs);
+    void update(int n);
+    // update() between CUDA events on the batch stream; returns the device ms
+    double update_timed(int n);
+    void sync();
+    int launches_per_iteration() const { return launches_; }
+    // sum over solves of 2 Ns M: gridpoint contour steps of one iteration
+    double gridpoint_steps_per_iteration() const;
+
+private:
+    struct Group {
+        int naxes = 0, Ns_max = 0;
+        std::vector<int> members;            // solve indices, Ns descending
+        std::vector<int> Ns;                  // Ns of members, same order
+        GroupSolve* dev = nullptr;            // descriptors on the device
+        int* prefix_dev[9] = {};              // CTA offsets per pass kind
+        std::vector<int> prefix[9];
+        size_t smem[9] = {};
+    };
+    void build_group(Group& g);
+    void enqueue_iteration();
+    std::vector<ModelAB*> m_;
+    std::vector<Group> groups_;
+    cudaStream_t st_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    int launches_ = 0;
+};
+
+}  // namespace ps

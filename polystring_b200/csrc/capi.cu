@@ -4,6 +4,7 @@
 #include "engine.h"
 #include "field_kernels.h"
 #include "string_ab.h"
+#include "batch_ab.h"
 
 #include <string>
 #include <vector>
@@ -54,6 +55,7 @@ using namespace ps;
 struct ps_updater { UpdaterCtx* ctx; };
 struct ps_model_ab { ModelAB* ctx; };
 struct ps_string_ab { StringAB* ctx; };
+struct ps_batch_ab { BatchAB* ctx; };
 
 extern "C" {
 
@@ -332,5 +334,81 @@ int ps_string_ab_synchronize(ps_string_ab* s) {
 }
 
 int ps_string_ab_launches_per_iteration(ps_string_ab* s) { return s ? s->ctx->launches_per_iteration() : -1; }
+
+int ps_batch_ab_create(const ps_model_ab_params* p, int n, ps_batch_ab** out) {
+    return guarded([&] {
+        if (!p || !out || n < 1) throw Error(PS_ERR_INVALID, "bad batch arguments");
+        std::vector<ModelABParams> ps;
+        for (int k = 0; k < n; k++) ps.push_back(to_params(p + k));
+        *out = new ps_batch_ab{new BatchAB(ps)};
+    });
+}
+
+void ps_batch_ab_destroy(ps_batch_ab* b) {
+    if (!b) return;
+    delete b->ctx;
+    delete b;
+}
+
+int ps_batch_ab_set_fields(ps_batch_ab* b, int k, const double* wA, const double* wB) {
+    return guarded([&] {
+        if (!b || !wA || !wB) throw Error(PS_ERR_INVALID, "null argument");
+        b->ctx->set_fields(k, wA, wB, false);
+    });
+}
+
+int ps_batch_ab_update(ps_batch_ab* b, int n_iter) {
+    return guarded([&] {
+        if (!b) throw Error(PS_ERR_INVALID, "null handle");
+        b->ctx->update(n_iter);
+    });
+}
+
+int ps_batch_ab_update_timed(ps_batch_ab* b, int n_iter, double* total_ms) {
+    return guarded([&] {
+        if (!b || !total_ms) throw Error(PS_ERR_INVALID, "null argument");
+        *total_ms = b->ctx->update_timed(n_iter);
+    });
+}
+
+int ps_batch_ab_H(ps_batch_ab* b, int k, double* H, double* Hw, double* Hs) {
+    return guarded([&] {
+        if (!b || !H || !Hw || !Hs) throw Error(PS_ERR_INVALID, "null argument");
+        b->ctx->sync();
+        b->ctx->model(k).H(H, Hw, Hs);
+    });
+}
+
+int ps_batch_ab_residual(ps_batch_ab* b, int k, double* res) {
+    return guarded([&] {
+        if (!b || !res) throw Error(PS_ERR_INVALID, "null argument");
+        b->ctx->sync();
+        *res = b->ctx->model(k).residual();
+    });
+}
+
+int ps_batch_ab_get(ps_batch_ab* b, int k, int which, double* out) {
+    return guarded([&] {
+        if (!b || !out) throw Error(PS_ERR_INVALID, "null argument");
+        b->ctx->sync();
+        b->ctx->model(k).get(which, out, false);
+    });
+}
+
+int ps_batch_ab_synchronize(ps_batch_ab* b) {
+    return guarded([&] {
+        if (!b) throw Error(PS_ERR_INVALID, "null handle");
+        b->ctx->sync();
+    });
+}
+
+int ps_batch_ab_launches_per_iteration(ps_batch_ab* b) { return b ? b->ctx->launches_per_iteration() : -1; }
+
+int ps_batch_ab_gridpoint_steps(ps_batch_ab* b, double* out) {
+    return guarded([&] {
+        if (!b || !out) throw Error(PS_ERR_INVALID, "null argument");
+        *out = b->ctx->gridpoint_steps_per_iteration();
+    });
+}
 
 }  // extern "C"

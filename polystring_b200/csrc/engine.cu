@@ -352,7 +352,7 @@ bool contour_weights(int rule, int n, std::vector<double>& c) {
 // ---------------------------------------------------------------------------
 // ModelAB
 // ---------------------------------------------------------------------------
-ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
+ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
     if (p.sA < 2 || p.sB < 2) throw Error(-1, "Ms must be at least [2, 2]");
     if (p.scft == 1 && (p.n_anderson < 1 || ax_nmax(p.n_anderson) == 0))
         throw Error(-2, "n_Anderson_mixing must be in 1..31");
@@ -394,7 +394,7 @@ ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
     }
     const char* force = getenv("PS_B200_LINE_PASSES");
     const char* generic = getenv("PS_B200_GENERIC_SWEEP");
-    const bool allow = !(force && force[0] == '1');
+    const bool allow = !(force && force[0] == '1') && !batch_member;
     use_sweep64_ = allow && p.mde == 0 && sweep64_supported(p.Lx, p.Ly, p.Lz) && !(generic && generic[0] == '1');
     use_sweep_ = allow && p.mde == 0 && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
     if (use_sweep64_) {
@@ -459,7 +459,7 @@ ModelAB::ModelAB(const ModelABParams& p) : p_(p) {
     launch_fill(hf_.p, M_, 1.0, st_);
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
-    if (!use_sweep_ && !use_sweep64_) chain_->autotune(st_);
+    if (!use_sweep_ && !use_sweep64_ && !batch_member) chain_->autotune(st_);
     PS_CUDA(cudaStreamSynchronize(st_));
     launches_per_prop_ = (use_sweep_ || use_sweep64_) ? 1 : chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
     launches_per_iter_ = launches_per_prop_ + 2 + 2 + (p.scft == 1 ? 4 : 1);
@@ -542,13 +542,13 @@ void ModelAB::enqueue_propagate() {
     chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, st_);
 }
 
-void ModelAB::enqueue_post() {
+void ModelAB::enqueue_post(cudaStream_t st) {
     // Q = qB->Qt() (Model_AB.cc:195, Propagator.cc:85-93)
     double* dQ = scal_.p + 0;
-    launch_mean(hf_.p + (long)Ns_ * M_, M_, partial_.p, dQ, st_);
+    launch_mean(hf_.p + (long)Ns_ * M_, M_, partial_.p, dQ, st);
     // phiA = (1/Q) dsA sum c_s qA[s] qAc[LA - s]; phiB likewise (Model_AB.cc:196-199)
-    launch_density(hf_.p, hc_.p + (long)LB_ * M_, LA_, M_, cA_.p, dsA_, dQ, 0.0, phiA_.p, 1, 0, 0, nullptr, st_);
-    launch_density(hf_.p + (long)LA_ * M_, hc_.p, LB_, M_, cB_.p, dsB_, dQ, 0.0, phiB_.p, 1, 0, 0, nullptr, st_);
+    launch_density(hf_.p, hc_.p + (long)LB_ * M_, LA_, M_, cA_.p, dsA_, dQ, 0.0, phiA_.p, 1, 0, 0, nullptr, st);
+    launch_density(hf_.p + (long)LA_ * M_, hc_.p, LB_, M_, cB_.p, dsB_, dQ, 0.0, phiB_.p, 1, 0, 0, nullptr, st);
     if (p_.scft == 1) {
         AXArgs a{};
         a.state = axs_; a.n = p_.n_anderson; a.M = M_;
@@ -557,14 +557,14 @@ void ModelAB::enqueue_post() {
         a.yita = yita_.p; a.chiN = p_.chiN; a.lamYita = p_.lamYita; a.dsA = dsA_; a.dsB = dsB_;
         a.compressible = p_.compressible;
         a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
-        launch_anderson(a, partial_.p, st_);
+        launch_anderson(a, partial_.p, st);
     } else {
         EMArgs a{};
         a.phiA = phiA_.p; a.phiB = phiB_.p; a.wA = wA_.p; a.wB = wB_.p; a.yita = yita_.p;
         a.M = M_; a.chiN = p_.chiN; a.lamA = p_.lamA; a.lamB = p_.lamB; a.lamYita = p_.lamYita;
         a.dsA = dsA_; a.dsB = dsB_; a.compressible = p_.compressible;
         a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p; a.bstride = 0;
-        launch_em_update(a, 1, st_);
+        launch_em_update(a, 1, st);
     }
 }
 

@@ -109,6 +109,11 @@ public:
     int launches_per_step() const;
     long M() const { return M_; }
     const AxisPlan& plan() const { return plan_; }
+    // work fields and tables (for grouped launches over many chains)
+    double2* z(int i) const { return z_[i].c(); }
+    double* u(int i) const { return u_[i].p; }
+    const double* L1() const { return L1_.p; }
+    const double* L2() const { return L2_.p; }
 
 private:
     int Lx_, Ly_, Lz_, scheme_, nbatch_;
@@ -129,7 +134,9 @@ struct ModelABParams {
 
 class ModelAB {
 public:
-    explicit ModelAB(const ModelABParams& p);
+    // batch_member: the propagators run in grouped launches of a BatchAB
+    // (line passes, no persistent sweep, no tile tuning of its own)
+    explicit ModelAB(const ModelABParams& p, bool batch_member = false);
     ~ModelAB();
     void set_fields(const double* wA, const double* wB, bool device_ptrs);
     void update(int n);
@@ -160,10 +167,23 @@ public:
     void forward_only();
     void grad_w(const double* phiA_bar, const double* phiB_bar, double Q_bar, double* gA, double* gB);
     void stress(double* dFdl);
+    // for BatchAB: the chain histories and factors, the post-propagator work
+    // (Q, densities, field update) on a given stream, and the iteration count
+    PairChain* chain() const { return chain_; }
+    double* hist_f() const { return hf_.p; }
+    double* hist_c() const { return hc_.p; }
+    const double* factor(int full, int block) const {
+        return full ? (block ? eFB_.p : eFA_.p) : (block ? eHB_.p : eHA_.p);
+    }
+    int LA() const { return LA_; }
+    int LB() const { return LB_; }
+    void enqueue_post(cudaStream_t s);
+    void advance(int n) { iter_ += n; }
+    bool has_fields() const { return fields_set_; }
 
 private:
     void enqueue_propagate();
-    void enqueue_post();
+    void enqueue_post() { enqueue_post(st_); }
     void ensure_graphs();
     void init_anderson(const double* wA, const double* wB, bool device_ptrs);
     void adjoint_weights(std::vector<double>& wAf, std::vector<double>& wBf) const;

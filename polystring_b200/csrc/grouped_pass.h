@@ -1,0 +1,42 @@
+// grouped_pass.h -- line passes of many independent propagator solves (of
+// different grids, contour lengths and block fractions) in one launch each.
+#pragma once
+
+#include "ps_internal.h"
+
+namespace ps {
+
+// One solve of a grouped launch: the paired chains of one Model_AB (lane f:
+// qA -> qB, lane c: qBc -> qAc), its work fields and tables, and its line
+// geometry.  Step t of the solve reads slice t of the histories and writes
+// slice t + 1; lane f is in block A for t < LA, lane c in block B for t < LB.
+struct GroupSolve {
+    LineGeom ax[3];
+    int naxes, Ns, LA, LB;
+    double M;
+    double* hf;
+    double* hc;
+    double2* z[3];
+    double* u[2];
+    const double* L1;
+    const double* L2;
+    const double* eF[2];        // e^{-w ds/2} of block A, block B
+    const double* eH[2];        // e^{-w ds/4}
+    const double2* tw[3];       // twiddles of each axis
+};
+
+// axis role of a pass: 0 = innermost (FIRST / MID / END), 1 = middle axis of
+// a 3D grid, 2 = outermost (OUTER)
+enum { GROUP_AX_IN = 0, GROUP_AX_MID = 1, GROUP_AX_OUT = 2 };
+
+bool grouped_size_supported(int N);
+void grouped_prepare();
+// CTAs of one solve in a pass of `mode` on axis role `ax` (p3: the single
+// field of the second half step)
+int grouped_ctas(const GroupSolve& s, int mode, int ax, int p3);
+// one grouped pass over solves[0 .. nactive): block b belongs to solve k when
+// prefix[k] <= b < prefix[k + 1]; smem = the largest tile any of them needs
+void grouped_launch(int mode, int ax, int p3, const GroupSolve* solves_dev, const int* prefix_dev, int nactive,
+                    int nblocks, size_t smem, int t, cudaStream_t st);
+
+}  // namespace ps
