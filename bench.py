@@ -188,6 +188,39 @@ def string_method(ps, iters=10):
             "timing": "host wall clock around synchronised replays"}
 
 
+def uneven_batch(ps, n=27, iters=2):
+    """Secondary result: C5-style independent solves of uneven grids and Ns
+    (a seeded sample of n solves) advanced as one batch, against the same
+    solves run one after another, each on its own fastest single path
+    (persistent sweeps on these cubic grids).  Device time by CUDA events."""
+    from polystring_b200 import workloads
+    specs = workloads.uneven_solves(n)
+
+    def model_args(sp):
+        return dict(dim=sp["dim"], shape=sp["shape"], cell=ps.make_cell(3, "CUBIC", sp["cell"][1][0]), Ms=sp["Ms"],
+                    chiN=sp["chiN"], lam=sp["lam"], scft=sp["scft"], n_anderson=sp["n_anderson"])
+    b = ps.BatchAB([model_args(sp) for sp in specs])
+    for k, sp in enumerate(specs):
+        b.set_fields(k, sp["wA"], sp["wB"])
+    b.update(1)
+    tb = b.update_timed(iters) / 1e3
+    work = b.gridpoint_steps() * iters
+    launches = b.launches_per_iteration()
+    del b
+    ts = 0.0
+    for sp in specs:
+        m = ps.ModelAB(**model_args(sp))
+        m.set_fields(sp["wA"], sp["wB"])
+        m.update(1)
+        ts += m.update_timed(iters)[0] / 1e3
+        del m
+    sizes = sorted({sp["shape"][0] for sp in specs})
+    return {"config": "C5 sample: %d solves, grids %s^3, Ns 64/128/256, Anderson(10), %d iterations" % (n, sizes, iters),
+            "batch_gridpt_steps_per_s": work / tb, "sequential_gridpt_steps_per_s": work / ts,
+            "speedup_vs_sequential": ts / tb, "launches_per_batch_iteration": launches,
+            "timing": "CUDA events on the batch stream / each solve's stream"}
+
+
 def run_reference(args, rank, world):
     """The reference algorithm's CPU restatement on all host threads (rank 0);
     each step is a bounded sample of the same workload."""
@@ -310,6 +343,7 @@ def main():
             "propagator_share_of_step": prop_s / total_s}
 
     string = string_method(ps) if rank == 0 and world == 1 else None
+    batch = uneven_batch(ps) if rank == 0 and world == 1 else None
 
     cpu = None
     if rank == 0 and world == 1:
@@ -324,7 +358,7 @@ def main():
                 "config": {"workload": WORKLOAD, "grid": list(shape), "Ns": Ns, "Ms": list(cfg["Ms"]),
                            "l2_flush": "inputs > L2 (0.8 GB histories)", "parallelism": "replicas" if world > 1 else "single"},
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clk.summary(), "H_after": H, "string_method": string}
+                "clocks": clk.summary(), "H_after": H, "string_method": string, "uneven_batch": batch}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

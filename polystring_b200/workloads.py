@@ -14,6 +14,7 @@ host and handed identically to the CUDA path and to the CPU oracle.
       2.0), each plus 0.05 N(0,1)
   C4  3D 48^3, orthorhombic (3.8, 4.0, 4.2), fA 0.30, chiN 22, Ns 128
       (Ms [39, 91])
+  C5  independent solves of uneven grids and Ns (uneven_solves)
 
 Ms follows from fA and Ns as LA = round(fA Ns), LB = Ns - LA, Ms = [LA+1, LB+1]
 (the reference reads Ms and recomputes f = LA/(LA+LB), src/Model_AB.cc:100-111).
@@ -73,6 +74,27 @@ def config(name, seed=2024):
                     lam=(0.05, 0.05, 5.0), mde="RQM4", scft="Anderson", n_anderson=20, iters=300,
                     wA=base[0], wB=base[1])
     raise KeyError(name)
+
+
+def uneven_solves(n=27, seed=2024):
+    """C5: independent solves on cubic grids {32^3, 48^3, 64^3} with Ns in
+    {64, 128, 256} (cycled, so every pairing occurs), fA ~ U(0.2, 0.5),
+    chiN ~ U(12, 30), cell ~ U(3.5, 5.0) Rg, Anderson mixing, fields
+    0.1 N(0, 1).  Ms follows from fA and Ns, so block lengths, and with them
+    Simpson or Quad4 rules, differ between solves."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        L = (32, 48, 64)[k % 3]
+        Ns = (64, 128, 256)[(k // 3) % 3]
+        fA = rng.uniform(0.2, 0.5)
+        chiN = rng.uniform(12.0, 30.0)
+        a = rng.uniform(3.5, 5.0)
+        shape = (L, L, L)
+        w = 0.1 * rng.standard_normal((2,) + shape)
+        out.append(dict(dim=3, shape=shape, cell=("CUBIC", (a,)), Ms=ms_from(fA, Ns), chiN=chiN,
+                        lam=(0.05, 0.05, 5.0), scft="Anderson", n_anderson=10, wA=w[0], wB=w[1]))
+    return out
 
 
 def string_images(m=40, shape=(128, 128, 1), L=8.0, seed=2024):
