@@ -261,22 +261,11 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def allmax(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from polystring_b200.dist import Ranks
+    ranks = Ranks("nccl")
+    dist = ranks.dist
+    barrier = ranks.barrier
+    allmax = ranks.allmax
 
     import polystring_b200 as ps
     cfg = config()
@@ -306,8 +295,9 @@ def main():
             print(json.dumps({"profile": True, "ms_per_step": total_s / args.steps * 1e3,
                               "propagator_ms_per_step": prop_ms / args.steps,
                               "launches_per_step": m.launches_per_iteration()}), flush=True)
+        ranks.close()
         return
-    value = world * units_per_step * args.steps / total_s
+    value = ranks.allsum(units_per_step * args.steps) / total_s
     launches = m.launches_per_iteration() * args.steps
     H = m.H()[0]
     if not np.isfinite(H):
@@ -360,9 +350,7 @@ def main():
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk.summary(), "H_after": H, "string_method": string, "uneven_batch": batch}
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
