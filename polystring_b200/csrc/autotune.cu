@@ -1,19 +1,22 @@
 // autotune.cu -- tile schedules of the line passes chosen by measurement.
 //
-// A line pass stages T lines of one axis in shared memory per CTA.  T sets
-// how many CTAs a pass has, how much shared memory each holds (so how many
-// are resident per SM) and how long the contiguous runs of the strided loads
-// are; which value is fastest depends on the grid, the batch and the scheme.
-// The tile height never changes the arithmetic of a line, so every candidate
-// gives bit-identical results and the choice is purely a timing question.
+// Two choices per axis.  The FFT schedule: the shared-memory Stockham radix
+// passes (any length), or the register-resident four-step (lengths 32..256,
+// fft_core.cuh RegPlan) compiled for one or for two resident CTAs per SM --
+// fewer registers and more warps against possible spills.  The tile height
+// of the Stockham passes: T lines per CTA sets the CTA count, the shared
+// memory per CTA (so the CTAs resident per SM) and the contiguous runs of the
+// strided loads.  Which is fastest depends on the grid, the batch and the
+// scheme.  The tile height never changes a line's arithmetic (bit-identical
+// results); the schedule changes only the order of the FFT's roundings.
 //
 // PairChain::autotune times complete contour steps of the chain's own pass
 // sequence (the enqueue() that the propagator graphs capture) on scratch
-// histories with unit fields, over tiles of 512, 1024 and 2048 elements per
-// axis that fit in shared memory, by coordinate descent over the axes (two
-// sweeps), keeping the fastest.  Results are cached per (grid, scheme, batch,
-// table layout) for the life of the process; PS_B200_AUTOTUNE=0 keeps the
-// default 2048-element tiles.
+// histories with unit fields, over Stockham tiles of 512, 1024 and 2048
+// elements and the register schedules, by coordinate descent over the axes
+// (two sweeps), keeping the fastest.  Results are cached per (grid, scheme,
+// batch, table layout) for the life of the process; PS_B200_AUTOTUNE=0 keeps
+// the defaults (Stockham passes, 2048-element tiles).
 #include "engine.h"
 #include "field_kernels.h"
 
@@ -31,7 +34,7 @@ namespace {
 
 using TuneKey = std::tuple<int, int, int, int, int, int>;
 std::mutex g_tune_mu;
-std::map<TuneKey, std::array<int, 3>> g_tune_cache;   // elements per tile of each axis
+std::map<TuneKey, std::array<int, 6>> g_tune_cache;   // elements per tile, then schedule, of each axis
 std::string g_tune_log;
 
 bool tuning_enabled() {
@@ -53,7 +56,10 @@ void PairChain::autotune(cudaStream_t st) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            for (int a = 0; a < plan_.naxes; a++) set_tile_elems(plan_.ax[a], it->second[a]);
+            for (int a = 0; a < plan_.naxes; a++) {
+                set_tile_elems(plan_.ax[a], it->second[a]);
+                plan_.ax[a].reg = it->second[3 + a];
+            }
             return;
         }
     }
@@ -92,36 +98,51 @@ void PairChain::autotune(cudaStream_t st) {
         return best;
     };
 
-    std::array<int, 3> choice = {2048, 2048, 2048};
-    for (int a = 0; a < plan_.naxes; a++) set_tile_elems(plan_.ax[a], choice[a]);
+    std::array<int, 3> choice = {2048, 2048, 2048}, sched = {0, 0, 0};
+    for (int a = 0; a < plan_.naxes; a++) {
+        set_tile_elems(plan_.ax[a], choice[a]);
+        sched[a] = plan_.ax[a].reg;
+    }
+    const std::array<int, 3> sched0 = sched;
     const float t_default = time_plan();
     float t_best = t_default;
     for (int sweep = 0; sweep < 2; sweep++) {
         for (int a = 0; a < plan_.naxes; a++) {
-            for (int c : cand) {
-                if (c == choice[a] || !fits(a, c)) continue;
-                set_tile_elems(plan_.ax[a], c);
-                const float t = time_plan();
-                if (t < 0.97f * t_best) {
-                    t_best = t;
-                    choice[a] = c;
+            const bool regok = reg_lines_per_cta(plan_.ax[a].N) > 0;
+            for (int r = 0; r <= (regok ? 2 : 0); r++) {
+                for (int c : cand) {
+                    if (r > 0 && c != choice[a]) continue;          // the tile matters to Stockham only
+                    if (r == sched[a] && c == choice[a]) continue;
+                    if (!fits(a, c)) continue;
+                    set_tile_elems(plan_.ax[a], c);
+                    plan_.ax[a].reg = r;
+                    const float t = time_plan();
+                    if (t < 0.97f * t_best) {
+                        t_best = t;
+                        choice[a] = c;
+                        sched[a] = r;
+                    }
                 }
             }
             set_tile_elems(plan_.ax[a], choice[a]);
+            plan_.ax[a].reg = sched[a];
         }
     }
     PS_CUDA(cudaEventDestroy(e0));
     PS_CUDA(cudaEventDestroy(e1));
     PS_CUDA(cudaStreamSynchronize(st));
 
-    char line[256];
-    std::snprintf(line, sizeof(line), "grid %dx%dx%d %s batch %d: tile elements [%d %d %d] T [%d %d %d], "
-                  "step %.1f us (default %.1f us)\n", Lx_, Ly_, Lz_, scheme_ == SCHEME_RQM4 ? "RQM4" : "OS2",
-                  nbatch_, choice[0], plan_.naxes > 1 ? choice[1] : 0, plan_.naxes > 2 ? choice[2] : 0,
-                  plan_.ax[0].T, plan_.naxes > 1 ? plan_.ax[1].T : 0, plan_.naxes > 2 ? plan_.ax[2].T : 0,
-                  1e3 * t_best / nst, 1e3 * t_default / nst);
+    static const char* names[3] = {"stockham", "reg4step", "reg4step-2cta"};
+    char line[320];
+    std::snprintf(line, sizeof(line), "grid %dx%dx%d %s batch %d: schedule [%s %s %s] tile elements [%d %d %d], "
+                  "step %.1f us (default [%s %s %s] %.1f us)\n", Lx_, Ly_, Lz_, scheme_ == SCHEME_RQM4 ? "RQM4" : "OS2",
+                  nbatch_, names[sched[0]], plan_.naxes > 1 ? names[sched[1]] : "-",
+                  plan_.naxes > 2 ? names[sched[2]] : "-", choice[0], plan_.naxes > 1 ? choice[1] : 0,
+                  plan_.naxes > 2 ? choice[2] : 0, 1e3 * t_best / nst, names[sched0[0]],
+                  plan_.naxes > 1 ? names[sched0[1]] : "-", plan_.naxes > 2 ? names[sched0[2]] : "-",
+                  1e3 * t_default / nst);
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    g_tune_cache[key] = choice;
+    g_tune_cache[key] = {choice[0], choice[1], choice[2], sched[0], sched[1], sched[2]};
     g_tune_log += line;
 }
 

@@ -15,6 +15,7 @@
 #include "batch_ab.h"
 
 #include <algorithm>
+#include <array>
 #include <numeric>
 
 namespace ps {
@@ -45,12 +46,22 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             m_.push_back(new ModelAB(p, true));
             if (m_.back()->chain()->plan().naxes < 2) throw Error(-2, "batched solves need 2D or 3D grids");
         }
-        for (int na = 2; na <= 3; na++) {
+        // groups: same number of long axes (the step's pass sequence) and the
+        // same schedule on each axis role (one kernel per grouped pass)
+        auto key = [&](int k) {
+            const AxisPlan& pl = m_[k]->chain()->plan();
+            return std::array<int, 4>{pl.naxes, pl.ax[0].reg, pl.naxes == 3 ? pl.ax[1].reg : 0,
+                                      pl.ax[pl.naxes - 1].reg};
+        };
+        std::vector<std::array<int, 4>> keys;
+        for (int k = 0; k < (int)m_.size(); k++)
+            if (std::find(keys.begin(), keys.end(), key(k)) == keys.end()) keys.push_back(key(k));
+        for (const auto& kk : keys) {
             Group g;
-            g.naxes = na;
+            g.naxes = kk[0];
+            g.path[0] = kk[1]; g.path[1] = kk[2]; g.path[2] = kk[3];
             for (int k = 0; k < (int)m_.size(); k++)
-                if (m_[k]->chain()->plan().naxes == na) g.members.push_back(k);
-            if (g.members.empty()) continue;
+                if (key(k) == kk) g.members.push_back(k);
             std::stable_sort(g.members.begin(), g.members.end(),
                              [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
             build_group(g);
@@ -128,8 +139,8 @@ void BatchAB::enqueue_iteration() {
             while (na < (int)g.Ns.size() && g.Ns[na] > t) na++;
             if (na == 0) continue;
             auto pass = [&](int k) {
-                grouped_launch(kPass[k][0], kPass[k][1], kPass[k][2], g.dev, g.prefix_dev[k], na, g.prefix[k][na],
-                               g.smem[k], t, st_);
+                grouped_launch(kPass[k][0], kPass[k][1], kPass[k][2], g.path[kPass[k][1]], g.dev, g.prefix_dev[k], na,
+                               g.prefix[k][na], g.smem[k], t, st_);
                 launches++;
             };
             const bool three = g.naxes == 3;

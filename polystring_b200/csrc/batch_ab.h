@@ -27,6 +27,7 @@ public:
 private:
     struct Group {
         int naxes = 0, Ns_max = 0;
+        int path[3] = {0, 0, 0};              // schedule of each axis role (in, mid, out)
         std::vector<int> members;            // solve indices, Ns descending
         std::vector<int> Ns;                  // Ns of members, same order
         GroupSolve* dev = nullptr;            // descriptors on the device

@@ -145,6 +145,8 @@ static int largest_divisor_le(long n, long cap) {
 }
 
 void set_tile_elems(LineGeom& g, int elems) {
+    const int lpc = reg_lines_per_cta(g.N);
+    g.rtiles = lpc > 0 ? (g.nlines + lpc - 1) / lpc : 0;
     const long target = std::max(1, elems / g.N);
     g.T = (g.S == 1) ? largest_divisor_le(g.nlines, target) : largest_divisor_le(g.S, target);
     g.LP = (g.S == 1 && g.T % 2 == 0) ? g.T + 1 : g.T;
@@ -170,6 +172,12 @@ AxisPlan make_axis_plan(int Lx, int Ly, int Lz) {
         g.S = strides[a];
         g.nlines = M / N;
         set_tile_elems(g, 2048);
+        // default schedule: Stockham passes (fastest in the measurements made
+        // so far); the autotuner tries the register-resident four-step where
+        // the length supports it; PS_B200_REG_FFT=0/1/2 forces a schedule
+        const char* rf = getenv("PS_B200_REG_FFT");
+        g.reg = 0;
+        if (rf && rf[0] >= '0' && rf[0] <= '2' && reg_lines_per_cta(N) > 0) g.reg = rf[0] - '0';
         ap.ax[ap.naxes++] = g;
     }
     if (ap.naxes == 0) throw Error(-2, "grid has no axis longer than one point");

@@ -115,6 +115,82 @@ template <int SIGN> struct Dft<8, SIGN> {
     }
 };
 
+template <int SIGN> struct Dft<16, SIGN> {
+    // 16 = 4 x 4: DFT4 over n1 of x[4 n1 + n2], twiddle W16^(n2 k1), DFT4
+    // over n2; X[k1 + 4 k2].  W16^m = cos(pi m/8) + sign i sin(pi m/8).
+    PS_HD static void run(double2* v) {
+        const double C1 = 0.92387953251128675613, S1 = 0.38268343236508977173;
+        double2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; n2++) {
+            double2 q[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            Dft<4, SIGN>::run(q);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; k1++) a[k1][n2] = q[k1];
+        }
+        const double sg = (double)SIGN;
+        // W^1, W^2, W^3, W^6, W^9 (W^4 = sign i)
+        const double2 w1 = mk(C1, sg * S1), w2 = mk(PS_SQRT1_2, sg * PS_SQRT1_2), w3 = mk(S1, sg * C1);
+        const double2 w6 = mk(-PS_SQRT1_2, sg * PS_SQRT1_2), w9 = mk(-C1, -sg * S1);
+        a[1][1] = cmul(a[1][1], w1); a[1][2] = cmul(a[1][2], w2); a[1][3] = cmul(a[1][3], w3);
+        a[2][1] = cmul(a[2][1], w2); a[2][2] = mul_si<SIGN>(a[2][2]); a[2][3] = cmul(a[2][3], w6);
+        a[3][1] = cmul(a[3][1], w3); a[3][2] = cmul(a[3][2], w6); a[3][3] = cmul(a[3][3], w9);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++) {
+            Dft<4, SIGN>::run(a[k1]);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = a[k1][k2];
+        }
+    }
+};
+
+// Register-resident line FFT (four-step, N = E x G): a line is owned by G
+// lanes of one warp, lane t holding the stride-G set x[G n + t], n < E.
+//   stage A (in registers): DFT_E over n, then twiddle W_N^(t k1);
+//   exchange (shared memory, one line's G lanes): lane t stores its E values
+//     at slots xslot(k1, t); lane t' then gathers (k1, t) for k1 = t' + G j;
+//   stage B (in registers): DFT_G over t for each j, giving X[k1 + E k2].
+// Lane t' ends with X[t' + G m], m = j + (E / G) k2: again the stride-G set
+// of offset t', so inverse transform, elementwise work and forward transform
+// chain without leaving registers.  The slot rotation (t + k1) mod G makes
+// both the stores and the gathers of a quarter-warp hit distinct bank groups.
+template <int N> struct RegPlan;
+template <> struct RegPlan<32>  { static constexpr int G = 4, E = 8, PAD = 4; };
+template <> struct RegPlan<64>  { static constexpr int G = 8, E = 8, PAD = 0; };
+template <> struct RegPlan<128> { static constexpr int G = 8, E = 16, PAD = 0; };
+template <> struct RegPlan<256> { static constexpr int G = 16, E = 16, PAD = 0; };
+
+template <int G> PS_HD int xslot(int k1, int t) { return k1 * G + ((t + k1) % G); }
+
+// stage A of lane t: tw[m] = W_N^m of the forward direction (conjugated for SIGN > 0)
+template <int N, int SIGN>
+PS_HD void reg_stage_a(double2* v, int t, const double2* tw) {
+    constexpr int E = RegPlan<N>::E;
+    Dft<E, SIGN>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < E; k1++) {
+        double2 w = tw[(t * k1) & (N - 1)];
+        if (SIGN > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+}
+
+// stage B of lane t from the exchange area of its line (after the stores)
+template <int N, int SIGN>
+PS_HD void reg_stage_b(double2* v, int t, const double2* line) {
+    constexpr int E = RegPlan<N>::E, G = RegPlan<N>::G;
+#pragma unroll
+    for (int j = 0; j < E / G; j++) {
+        double2 w[G];
+        const int k1 = t + G * j;
+#pragma unroll
+        for (int s = 0; s < G; s++) w[s] = line[xslot<G>(k1, s)];
+        Dft<G, SIGN>::run(w);
+#pragma unroll
+        for (int k2 = 0; k2 < G; k2++) v[j + (E / G) * k2] = w[k2];
+    }
+}
+
 // Radix plans per line length (compile time).  Every supported length is
 // 2^a 3^b with at most three passes.
 template <int N> struct Plan;

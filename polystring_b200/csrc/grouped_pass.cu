@@ -24,30 +24,43 @@ __device__ __forceinline__ int find_solve(const int* __restrict__ prefix, int n,
     return lo;
 }
 
-template <int MODE>
+// PATH 0: Stockham body for every supported length; PATH 1 / 2: the
+// register-resident body (lengths 32, 64, 128), compiled into separate
+// kernels so that each keeps its own register budget
+template <int MODE, int PATH>
 __device__ __forceinline__ void dispatch_n(const LineGeom& g, const StepPtrs& p, const double2* tw, long tile, int fy) {
-    switch (g.N) {
-    case 16: line_pass_body<16, MODE>(g, p, tw, tile, fy, 0); break;
-    case 24: line_pass_body<24, MODE>(g, p, tw, tile, fy, 0); break;
-    case 32: line_pass_body<32, MODE>(g, p, tw, tile, fy, 0); break;
-    case 48: line_pass_body<48, MODE>(g, p, tw, tile, fy, 0); break;
-    case 64: line_pass_body<64, MODE>(g, p, tw, tile, fy, 0); break;
-    case 96: line_pass_body<96, MODE>(g, p, tw, tile, fy, 0); break;
-    case 128: line_pass_body<128, MODE>(g, p, tw, tile, fy, 0); break;
-    default: break;   // rejected on the host (grouped_size_supported)
+    if constexpr (PATH == 0) {
+        switch (g.N) {
+        case 16: line_pass_body<16, MODE>(g, p, tw, tile, fy, 0); break;
+        case 24: line_pass_body<24, MODE>(g, p, tw, tile, fy, 0); break;
+        case 32: line_pass_body<32, MODE>(g, p, tw, tile, fy, 0); break;
+        case 48: line_pass_body<48, MODE>(g, p, tw, tile, fy, 0); break;
+        case 64: line_pass_body<64, MODE>(g, p, tw, tile, fy, 0); break;
+        case 96: line_pass_body<96, MODE>(g, p, tw, tile, fy, 0); break;
+        case 128: line_pass_body<128, MODE>(g, p, tw, tile, fy, 0); break;
+        default: break;   // rejected on the host (grouped_size_supported)
+        }
+    } else {
+        switch (g.N) {
+        case 32: line_pass_body_reg<32, MODE>(g, p, tw, tile, fy, 0); break;
+        case 64: line_pass_body_reg<64, MODE>(g, p, tw, tile, fy, 0); break;
+        case 128: line_pass_body_reg<128, MODE>(g, p, tw, tile, fy, 0); break;
+        default: break;   // the host groups only register-capable lengths here
+        }
     }
 }
 
-template <int MODE, int AX, int P3>
-__global__ void __launch_bounds__(kThreads) grouped_pass_kernel(const GroupSolve* __restrict__ solves,
-                                                                const int* __restrict__ prefix, int nactive, int t) {
+template <int MODE, int AX, int P3, int PATH>
+__global__ void __launch_bounds__(kThreads, PATH == 2 ? 2 : 1)
+    grouped_pass_kernel(const GroupSolve* __restrict__ solves, const int* __restrict__ prefix, int nactive, int t) {
     const int s = find_solve(prefix, nactive, blockIdx.x);
     const GroupSolve& D = solves[s];
     const int a = AX == GROUP_AX_IN ? 0 : (AX == GROUP_AX_MID ? 1 : D.naxes - 1);
     const LineGeom g = D.ax[a];
     const int local = blockIdx.x - prefix[s];
-    const long tile = local % g.ntiles;
-    const int fy = local / g.ntiles;
+    const long nt = pass_tiles(g, MODE);
+    const long tile = local % nt;
+    const int fy = (int)(local / nt);
     const long M = (long)D.M;
     StepPtrs p{};
     p.M = D.M;
@@ -71,35 +84,43 @@ __global__ void __launch_bounds__(kThreads) grouped_pass_kernel(const GroupSolve
         p.z[0] = D.z[2];
         p.L[0] = D.L2;
     }
-    dispatch_n<MODE>(g, p, D.tw[a], tile, fy);
+    dispatch_n<MODE, PATH>(g, p, D.tw[a], tile, fy);
 }
 
-template <int MODE, int AX, int P3>
+template <int MODE, int AX, int P3, int PATH>
 void launch_one(const GroupSolve* s, const int* prefix, int nactive, int nblocks, size_t smem, int t, cudaStream_t st,
                 bool prepare) {
     if (prepare) {
-        PS_CUDA(cudaFuncSetAttribute(grouped_pass_kernel<MODE, AX, P3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)kLinePassSmemLimit));
+        PS_CUDA(cudaFuncSetAttribute(grouped_pass_kernel<MODE, AX, P3, PATH>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLinePassSmemLimit));
         return;
     }
-    grouped_pass_kernel<MODE, AX, P3><<<nblocks, kThreads, smem, st>>>(s, prefix, nactive, t);
+    grouped_pass_kernel<MODE, AX, P3, PATH><<<nblocks, kThreads, smem, st>>>(s, prefix, nactive, t);
     PS_CUDA(cudaGetLastError());
 }
 
-void dispatch(int mode, int ax, int p3, const GroupSolve* s, const int* prefix, int nactive, int nblocks, size_t smem,
-              int t, cudaStream_t st, bool prepare) {
-    if (mode == MODE_FIRST_RQM4 && ax == GROUP_AX_IN) return launch_one<MODE_FIRST_RQM4, 0, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
-    if (mode == MODE_MID_RQM4 && ax == GROUP_AX_IN) return launch_one<MODE_MID_RQM4, 0, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
-    if (mode == MODE_END_RQM4 && ax == GROUP_AX_IN) return launch_one<MODE_END_RQM4, 0, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+template <int MODE, int AX, int P3>
+void launch_path(int path, const GroupSolve* s, const int* prefix, int nactive, int nblocks, size_t smem, int t,
+                 cudaStream_t st, bool prepare) {
+    if (path == 1) return launch_one<MODE, AX, P3, 1>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+    if (path == 2) return launch_one<MODE, AX, P3, 2>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+    return launch_one<MODE, AX, P3, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+}
+
+void dispatch(int mode, int ax, int p3, int path, const GroupSolve* s, const int* prefix, int nactive, int nblocks,
+              size_t smem, int t, cudaStream_t st, bool prepare) {
+    if (mode == MODE_FIRST_RQM4 && ax == GROUP_AX_IN) return launch_path<MODE_FIRST_RQM4, 0, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
+    if (mode == MODE_MID_RQM4 && ax == GROUP_AX_IN) return launch_path<MODE_MID_RQM4, 0, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
+    if (mode == MODE_END_RQM4 && ax == GROUP_AX_IN) return launch_path<MODE_END_RQM4, 0, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
     if (mode == MODE_FWD && ax == GROUP_AX_MID)
-        return p3 ? launch_one<MODE_FWD, 1, 1>(s, prefix, nactive, nblocks, smem, t, st, prepare)
-                  : launch_one<MODE_FWD, 1, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+        return p3 ? launch_path<MODE_FWD, 1, 1>(path, s, prefix, nactive, nblocks, smem, t, st, prepare)
+                  : launch_path<MODE_FWD, 1, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
     if (mode == MODE_INV && ax == GROUP_AX_MID)
-        return p3 ? launch_one<MODE_INV, 1, 1>(s, prefix, nactive, nblocks, smem, t, st, prepare)
-                  : launch_one<MODE_INV, 1, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+        return p3 ? launch_path<MODE_INV, 1, 1>(path, s, prefix, nactive, nblocks, smem, t, st, prepare)
+                  : launch_path<MODE_INV, 1, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
     if (mode == MODE_OUTER && ax == GROUP_AX_OUT)
-        return p3 ? launch_one<MODE_OUTER, 2, 1>(s, prefix, nactive, nblocks, smem, t, st, prepare)
-                  : launch_one<MODE_OUTER, 2, 0>(s, prefix, nactive, nblocks, smem, t, st, prepare);
+        return p3 ? launch_path<MODE_OUTER, 2, 1>(path, s, prefix, nactive, nblocks, smem, t, st, prepare)
+                  : launch_path<MODE_OUTER, 2, 0>(path, s, prefix, nactive, nblocks, smem, t, st, prepare);
     throw Error(-1, "no grouped pass for this mode and axis");
 }
 
@@ -116,7 +137,8 @@ void grouped_prepare() {
     const int modes[][3] = {{MODE_FIRST_RQM4, 0, 0}, {MODE_MID_RQM4, 0, 0}, {MODE_END_RQM4, 0, 0},
                             {MODE_FWD, 1, 0},        {MODE_FWD, 1, 1},      {MODE_INV, 1, 0},
                             {MODE_INV, 1, 1},        {MODE_OUTER, 2, 0},    {MODE_OUTER, 2, 1}};
-    for (auto& m : modes) dispatch(m[0], m[1], m[2], nullptr, nullptr, 0, 0, 0, 0, 0, true);
+    for (auto& m : modes)
+        for (int path = 0; path < 3; path++) dispatch(m[0], m[1], m[2], path, nullptr, nullptr, 0, 0, 0, 0, 0, true);
     for (int N : {16, 24, 32, 48, 64, 96, 128}) twiddle_table(N);
 }
 
@@ -125,13 +147,13 @@ int grouped_ctas(const GroupSolve& s, int mode, int ax, int p3) {
     int gy = 1;
     if (mode == MODE_FIRST_RQM4 || mode == MODE_MID_RQM4) gy = 2;
     if (mode == MODE_FWD || mode == MODE_INV || mode == MODE_OUTER) gy = p3 ? 1 : 2;
-    return (int)s.ax[a].ntiles * gy;
+    return (int)pass_tiles(s.ax[a], mode) * gy;
 }
 
-void grouped_launch(int mode, int ax, int p3, const GroupSolve* solves_dev, const int* prefix_dev, int nactive,
-                    int nblocks, size_t smem, int t, cudaStream_t st) {
+void grouped_launch(int mode, int ax, int p3, int path, const GroupSolve* solves_dev, const int* prefix_dev,
+                    int nactive, int nblocks, size_t smem, int t, cudaStream_t st) {
     if (nactive <= 0 || nblocks <= 0) return;
-    dispatch(mode, ax, p3, solves_dev, prefix_dev, nactive, nblocks, smem, t, st, false);
+    dispatch(mode, ax, p3, path, solves_dev, prefix_dev, nactive, nblocks, smem, t, st, false);
 }
 
 }  // namespace ps

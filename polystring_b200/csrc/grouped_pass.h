@@ -36,7 +36,9 @@ void grouped_prepare();
 int grouped_ctas(const GroupSolve& s, int mode, int ax, int p3);
 // one grouped pass over solves[0 .. nactive): block b belongs to solve k when
 // prefix[k] <= b < prefix[k + 1]; smem = the largest tile any of them needs
-void grouped_launch(int mode, int ax, int p3, const GroupSolve* solves_dev, const int* prefix_dev, int nactive,
-                    int nblocks, size_t smem, int t, cudaStream_t st);
+// path: the schedule of the pass's axis in every solve of the launch (LineGeom::reg; 1 and 2 only
+// for lengths 32, 64, 128)
+void grouped_launch(int mode, int ax, int p3, int path, const GroupSolve* solves_dev, const int* prefix_dev,
+                    int nactive, int nblocks, size_t smem, int t, cudaStream_t st);
 
 }  // namespace ps

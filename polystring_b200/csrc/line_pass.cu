@@ -29,6 +29,15 @@ __global__ void __launch_bounds__(kThreads) line_pass_kernel(LineGeom g, StepPtr
     line_pass_body<N, MODE>(g, p, gtw, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// register-resident passes, compiled apart from the Stockham ones so that
+// each keeps its own register budget; OCC = resident CTAs per SM the
+// compiler must allow (1: no spills, 2: twice the warps, may spill at 128+)
+template <int N, int MODE, int OCC>
+__global__ void __launch_bounds__(kThreads, OCC)
+    line_pass_reg_kernel(LineGeom g, StepPtrs p, const double2* __restrict__ gtw) {
+    if constexpr (reg_body<N, MODE>()) line_pass_body_reg<N, MODE>(g, p, gtw, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 constexpr int kMaxSmem = (int)kLinePassSmemLimit;
 
 int buffers_for_mode(int mode) {
@@ -51,6 +60,12 @@ template <int N, int MODE>
 void prepare_nm() {
     PS_CUDA(cudaFuncSetAttribute(line_pass_kernel<N, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kMaxSmem));
+    if constexpr (reg_body<N, MODE>()) {
+        PS_CUDA(cudaFuncSetAttribute(line_pass_reg_kernel<N, MODE, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kMaxSmem));
+        PS_CUDA(cudaFuncSetAttribute(line_pass_reg_kernel<N, MODE, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kMaxSmem));
+    }
 }
 
 template <int N, int MODE>
@@ -58,7 +73,19 @@ void launch_nm(const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st
     if (prepare_only) { prepare_nm<N, MODE>(); return; }
     size_t smem = line_pass_smem_bytes(MODE, g);
     if (smem > (size_t)kMaxSmem) throw Error(-2, "line pass tile does not fit in shared memory");
-    dim3 grid((unsigned)g.ntiles, (unsigned)grid_y_for_mode(MODE, p.nfield), (unsigned)nbatch);
+    dim3 grid((unsigned)pass_tiles(g, MODE), (unsigned)grid_y_for_mode(MODE, p.nfield), (unsigned)nbatch);
+    if constexpr (reg_body<N, MODE>()) {
+        if (g.reg == 1) {
+            line_pass_reg_kernel<N, MODE, 1><<<grid, kThreads, smem, st>>>(g, p, twiddle_table(N));
+            PS_CUDA(cudaGetLastError());
+            return;
+        }
+        if (g.reg == 2) {
+            line_pass_reg_kernel<N, MODE, 2><<<grid, kThreads, smem, st>>>(g, p, twiddle_table(N));
+            PS_CUDA(cudaGetLastError());
+            return;
+        }
+    }
     line_pass_kernel<N, MODE><<<grid, kThreads, smem, st>>>(g, p, twiddle_table(N));
     PS_CUDA(cudaGetLastError());
 }
@@ -113,6 +140,11 @@ void dispatch(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaSt
 }  // namespace
 
 size_t line_pass_smem_bytes(int mode, const LineGeom& g) {
+    if (g.reg && reg_mode(mode)) {
+        // twiddles + one exchange area per line of the CTA (RegPlan pads N = 32)
+        const size_t ls = g.N + (g.N == 32 ? 4 : 0);
+        return sizeof(double2) * ((size_t)g.N + (size_t)reg_lines_per_cta(g.N) * ls);
+    }
     return sizeof(double2) * (2 * (size_t)g.N + (size_t)buffers_for_mode(mode) * g.N * g.LP);
 }
 

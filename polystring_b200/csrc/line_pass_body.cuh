@@ -389,5 +389,202 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
     }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident passes (power-of-two lengths 32..256): a line belongs to
+// G lanes of one warp (RegPlan<N>), each warp handles 32/G lines, and a CTA's
+// warps are independent -- the only shared-memory traffic is one swizzled
+// exchange per transform, synchronised with __syncwarp.  Lanes of lines past
+// the end of the field still take part in every exchange (their loads and
+// stores are skipped), so the warp-wide synchronisation stays complete.
+// ---------------------------------------------------------------------------
+template <int N>
+constexpr bool reg_capable() { return N == 32 || N == 64 || N == 128 || N == 256; }
+
+template <int N, int MODE>
+constexpr bool reg_body() {
+    return reg_capable<N>() && (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_OUTER ||
+                                MODE == MODE_FIRST_RQM4 || MODE == MODE_MID_RQM4 || MODE == MODE_END_RQM4);
+}
+
+template <int N, int SIGN>
+__device__ __forceinline__ void reg_fft(double2 (&v)[RegPlan<N>::E], int t, double2* xbuf, const double2* tw) {
+    constexpr int E = RegPlan<N>::E, G = RegPlan<N>::G;
+    reg_stage_a<N, SIGN>(v, t, tw);
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < E; k1++) xbuf[xslot<G>(k1, t)] = v[k1];
+    __syncwarp();
+    reg_stage_b<N, SIGN>(v, t, xbuf);
+}
+
+template <int N, int MODE>
+__device__ __forceinline__ void line_pass_body_reg(const LineGeom& g, const StepPtrs& p,
+                                                   const double2* __restrict__ gtw, const long cta, const int fy,
+                                                   const long bz) {
+    constexpr int G = RegPlan<N>::G, E = RegPlan<N>::E, LS = N + RegPlan<N>::PAD, LW = 32 / G;
+    extern __shared__ double2 smem[];
+    double2* tw = smem;
+    for (int m = threadIdx.x; m < N; m += blockDim.x) tw[m] = gtw[m];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lw = lane / G, t = lane % G;
+    double2* xbuf = smem + N + (warp * LW + lw) * LS;
+    const long line = (cta * (kThreads / 32) + warp) * LW + lw;
+    const bool valid = line < g.nlines;
+    long base = 0, ns = 1;
+    if (g.S == 1) {
+        base = line * N;
+    } else {
+        const long o = line / g.S, i0 = line - o * g.S;
+        base = o * (long)N * g.S + i0;
+        ns = g.S;
+    }
+    const double M = p.M;
+    const double rM = 1.0 / M;
+    const long oz = bz * p.bstride_z, oq = bz * p.bstride_q, oe = bz * p.bstride_e, oL = bz * p.bstride_L;
+    const long ou = bz * p.bstride_u;
+    // register m of every lane holds element t + G m of its line
+    auto off = [&](int m) { return base + (long)(t + G * m) * ns; };
+    double2 v[E];
+
+    if constexpr (MODE == MODE_FWD || MODE == MODE_INV || MODE == MODE_OUTER) {
+        double2* z = p.z[fy] + oz;
+#pragma unroll
+        for (int m = 0; m < E; m++) v[m] = valid ? z[off(m)] : make_double2(0.0, 0.0);
+        if constexpr (MODE == MODE_INV) {
+            reg_fft<N, +1>(v, t, xbuf, tw);
+        } else {
+            reg_fft<N, -1>(v, t, xbuf, tw);
+        }
+        if constexpr (MODE == MODE_OUTER) {
+            if (p.spec[fy] && valid) {
+                double2* sp = p.spec[fy] + oz;
+#pragma unroll
+                for (int m = 0; m < E; m++) sp[off(m)] = v[m];
+            }
+            const double* L = p.L[fy] + oL;
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                const double lv = valid ? L[off(m)] : 0.0;
+                v[m] = make_double2(v[m].x * lv, v[m].y * lv);
+            }
+            reg_fft<N, +1>(v, t, xbuf, tw);
+        }
+        if (valid) {
+#pragma unroll
+            for (int m = 0; m < E; m++) z[off(m)] = v[m];
+        }
+    } else if constexpr (MODE == MODE_FIRST_RQM4) {
+        const double* ef = (fy == 0 ? p.eF[0] : p.eH[0]) + oe;
+        const double* ec = (fy == 0 ? p.eF[1] : p.eH[1]) + oe;
+        const double* qf = p.qin[0] + oq;
+        const double* qc = p.qin[1] + oq;
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            if (valid) {
+                const long i = off(m);
+                v[m] = make_double2(ef[i] * qf[i], ec[i] * qc[i]);
+            } else {
+                v[m] = make_double2(0.0, 0.0);
+            }
+        }
+        reg_fft<N, -1>(v, t, xbuf, tw);
+        if (valid) {
+            double2* z = p.z[fy] + oz;
+#pragma unroll
+            for (int m = 0; m < E; m++) z[off(m)] = v[m];
+        }
+    } else if constexpr (MODE == MODE_MID_RQM4) {
+        const double2* zin = p.z[fy == 0 ? 0 : 1] + oz;
+#pragma unroll
+        for (int m = 0; m < E; m++) v[m] = valid ? zin[off(m)] : make_double2(0.0, 0.0);
+        reg_fft<N, +1>(v, t, xbuf, tw);
+        if (fy == 0) {
+            // full step: u = Re/Im(F^-1 Z1) e^{-w ds/2} / M
+            const double* ef = p.eF[0] + oe;
+            const double* ec = p.eF[1] + oe;
+            if (valid) {
+#pragma unroll
+                for (int m = 0; m < E; m++) {
+                    const long i = off(m);
+                    p.u[0][ou + i] = div_rn(v[m].x * ef[i], M, rM);
+                    p.u[1][ou + i] = div_rn(v[m].y * ec[i], M, rM);
+                }
+            }
+        } else {
+            // first half step finishes, second half step starts
+            const double* hf = p.eH[0] + oe;
+            const double* hc = p.eH[1] + oe;
+#pragma unroll
+            for (int m = 0; m < E; m++) {
+                if (valid) {
+                    const long i = off(m);
+                    const double a = hf[i], b = hc[i];
+                    const double qtf = div_rn(v[m].x * a, M, rM);
+                    const double qtc = div_rn(v[m].y * b, M, rM);
+                    if (p.half[0]) {
+                        p.half[0][ou + i] = qtf;
+                        p.half[1][ou + i] = qtc;
+                    }
+                    v[m] = make_double2(a * qtf, b * qtc);
+                } else {
+                    v[m] = make_double2(0.0, 0.0);
+                }
+            }
+            reg_fft<N, -1>(v, t, xbuf, tw);
+            if (valid) {
+                double2* z3 = p.z[2] + oz;
+#pragma unroll
+                for (int m = 0; m < E; m++) z3[off(m)] = v[m];
+            }
+        }
+    } else if constexpr (MODE == MODE_END_RQM4) {
+        const double2* zin = p.z[2] + oz;
+#pragma unroll
+        for (int m = 0; m < E; m++) v[m] = valid ? zin[off(m)] : make_double2(0.0, 0.0);
+        reg_fft<N, +1>(v, t, xbuf, tw);
+        const double* hf = p.eH[0] + oe;
+        const double* hc = p.eH[1] + oe;
+        double2 q[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            if (valid) {
+                const long i = off(m);
+                double qf = div_rn(v[m].x * hf[i], M, rM);
+                double qc = div_rn(v[m].y * hc[i], M, rM);
+                qf = div_rn(4.0 * qf - p.u[0][ou + i], 3.0, 1.0 / 3.0);
+                qc = div_rn(4.0 * qc - p.u[1][ou + i], 3.0, 1.0 / 3.0);
+                p.qout[0][oq + i] = qf;
+                p.qout[1][oq + i] = qc;
+                q[m] = make_double2(qf, qc);
+            } else {
+                q[m] = make_double2(0.0, 0.0);
+            }
+        }
+        if (p.chain_next) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const double* nf = (k == 0 ? p.nF[0] : p.nH[0]) + oe;
+                const double* nc = (k == 0 ? p.nF[1] : p.nH[1]) + oe;
+#pragma unroll
+                for (int m = 0; m < E; m++) {
+                    if (valid) {
+                        const long i = off(m);
+                        v[m] = make_double2(nf[i] * q[m].x, nc[i] * q[m].y);
+                    } else {
+                        v[m] = make_double2(0.0, 0.0);
+                    }
+                }
+                reg_fft<N, -1>(v, t, xbuf, tw);
+                if (valid) {
+                    double2* z = p.z[k] + oz;
+#pragma unroll
+                    for (int m = 0; m < E; m++) z[off(m)] = v[m];
+                }
+            }
+        }
+    }
+}
+
 }  // namespace lp
 }  // namespace ps

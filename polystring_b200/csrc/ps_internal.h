@@ -51,7 +51,23 @@ struct LineGeom {
     long nlines;  // lines per field (M / N)
     long ntiles;  // tiles per field (nlines / T)
     int tshift;   // log2(T) when T is a power of two, else -1
+    int reg;      // schedule of the RQM4 / FFT passes of this axis: 0 Stockham in shared memory,
+                  // 1 register-resident four-step (one CTA per SM), 2 the same at two CTAs per SM
+    long rtiles;  // CTAs per field of a register-resident pass
 };
+
+// Register-resident line FFT (fft_core.cuh RegPlan): lines per 256-thread
+// CTA for the supported lengths (0 = not supported), and the pass modes that
+// have a register-resident body.
+__host__ __device__ inline int reg_lines_per_cta(int N) {
+    switch (N) {
+    case 32: return 64;
+    case 64: return 32;
+    case 128: return 32;
+    case 256: return 16;
+    default: return 0;
+    }
+}
 
 // Pointers used by the fused first / last passes.  A "lane" is one of the
 // two real chains packed into one complex field: lane f in the real part,
@@ -85,6 +101,13 @@ struct StepPtrs {
     double wdA, wdB;
     const double* next_qf;   // END_ADJ chaining: lane f input of the next step
 };
+
+__host__ __device__ inline bool reg_mode(int mode) {
+    return mode == MODE_FWD || mode == MODE_INV || mode == MODE_OUTER || mode == MODE_FIRST_RQM4 ||
+           mode == MODE_MID_RQM4 || mode == MODE_END_RQM4;
+}
+// CTAs per field of a pass of `mode` on axis g
+__host__ __device__ inline long pass_tiles(const LineGeom& g, int mode) { return (g.reg && reg_mode(mode)) ? g.rtiles : g.ntiles; }
 
 void launch_line_pass(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaStream_t st);
 // sets kernel attributes and builds twiddles; call outside stream capture

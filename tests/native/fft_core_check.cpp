@@ -73,8 +73,47 @@ static double check_div() {
     return (double)bad;
 }
 
+// the register-resident four-step FFT, every lane emulated in turn: stage A,
+// the swizzled stores, stage B; against the long-double DFT
+template <int N, int SIGN>
+static double run_reg() {
+    constexpr int E = ps::RegPlan<N>::E, G = ps::RegPlan<N>::G;
+    std::vector<double2> x(N), tw(N), line(E * G);
+    for (int i = 0; i < N; i++) {
+        x[i] = ps::mk(std::sin(0.37 * i + 0.1) + 0.25 * i / N, std::cos(1.3 * i) - 0.5);
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * i / N;
+        tw[i] = ps::mk((double)cosl(a), (double)sinl(a));
+    }
+    std::vector<std::vector<double2>> v(G, std::vector<double2>(E));
+    for (int t = 0; t < G; t++) {
+        for (int n = 0; n < E; n++) v[t][n] = x[G * n + t];
+        ps::reg_stage_a<N, SIGN>(v[t].data(), t, tw.data());
+        for (int k1 = 0; k1 < E; k1++) line[ps::xslot<G>(k1, t)] = v[t][k1];
+    }
+    double err = 0, mx = 0;
+    for (int t = 0; t < G; t++) {
+        ps::reg_stage_b<N, SIGN>(v[t].data(), t, line.data());
+        for (int m = 0; m < E; m++) {
+            const int k = t + G * m;
+            long double re = 0, im = 0;
+            for (int n = 0; n < N; n++) {
+                long double a = SIGN * 2.0L * 3.14159265358979323846264338327950288L * ((long)k * n % N) / N;
+                re += x[n].x * cosl(a) - x[n].y * sinl(a);
+                im += x[n].x * sinl(a) + x[n].y * cosl(a);
+            }
+            err = fmax(err, fmax(fabs((double)(v[t][m].x - re)), fabs((double)(v[t][m].y - im))));
+            mx = fmax(mx, fmax(fabs((double)re), fabs((double)im)));
+        }
+    }
+    printf("reg%d %d %.3e\n", N, SIGN, err / mx);
+    return err / mx;
+}
+
 int main() {
     double e = check_div();
+    e = fmax(e, run_reg<32, -1>()); e = fmax(e, run_reg<64, -1>()); e = fmax(e, run_reg<128, -1>());
+    e = fmax(e, run_reg<256, -1>()); e = fmax(e, run_reg<32, 1>()); e = fmax(e, run_reg<128, 1>());
+    e = fmax(e, run_reg<256, 1>());
     e = fmax(e, run<2, -1>());   e = fmax(e, run<4, -1>());   e = fmax(e, run<8, -1>());
     e = fmax(e, run<12, -1>());  e = fmax(e, run<16, -1>());  e = fmax(e, run<24, -1>());
     e = fmax(e, run<32, -1>());  e = fmax(e, run<48, -1>());  e = fmax(e, run<64, -1>());

@@ -47,7 +47,9 @@ def _spec(ps, s):
     return dict(dim=dim, shape=shape, cell=_cell(ps, dim, L), Ms=Ms, chiN=chiN, scft=scft, n_anderson=4)
 
 
-def test_batch_members_follow_their_single_solves_exactly(ps):
+def test_batch_members_follow_their_single_solves_exactly(ps, monkeypatch):
+    # batch members run the default FFT schedules; untuned single solves do too
+    monkeypatch.setenv("PS_B200_AUTOTUNE", "0")
     b = ps.BatchAB([_spec(ps, s) for s in SOLVES])
     singles = []
     for k, s in enumerate(SOLVES):
