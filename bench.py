@@ -221,6 +221,74 @@ def uneven_batch(ps, n=27, iters=2):
             "timing": "CUDA events on the batch stream / each solve's stream"}
 
 
+def adjoint_c4(ps, iters=120):
+    """Secondary result: the adjoint on C4 (48^3 orthorhombic (3.8, 4.0, 4.2),
+    fA 0.30, chiN 22, Ns 128, seeded start relaxed by Anderson iterations):
+    time of one stress evaluation (dF/dL_cell) and of one loss gradient
+    (Loss = ||phiA - phi_target||^2, phi_target a smoothed seeded field in
+    [0, 1]), each including its forward map, and their agreement with fourth-
+    order central differences of the forward map (h = 1e-4)."""
+    from polystring_b200 import workloads
+    cfg = workloads.config("C4")
+    L = cfg["cell"][1]
+    mk = lambda l: ps.make_cell(3, "ORTHORHOMBIC", *l)
+    m = ps.ModelAB(3, cfg["shape"], mk(L), cfg["Ms"], cfg["chiN"], lam=cfg["lam"], scft="Anderson", n_anderson=20)
+    m.set_fields(cfg["wA"], cfg["wB"])
+    m.update(iters)
+    res = m.residual_error()
+    wA, wB = m.get("wA"), m.get("wB")
+    rng = np.random.default_rng(7)
+    tgt = rng.uniform(0, 1, cfg["shape"])
+    for _ in range(2):                       # smooth the target (periodic 3-point means)
+        tgt = sum(np.roll(tgt, s, ax) for ax in range(3) for s in (-1, 0, 1)) / 9.0
+    m.set_fields(wA, wB)
+    st = m.stress()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        st = m.stress()
+    t_stress = (time.perf_counter() - t0) / 3
+    m.forward()
+    phi = m.get("phiA")
+    t0 = time.perf_counter()
+    for _ in range(3):
+        gA, gB = m.grad_w(2.0 * (phi - tgt), np.zeros(cfg["shape"]), 0.0)
+    t_grad = (time.perf_counter() - t0) / 3
+    h = 1e-4
+    err_s = 0.0
+    for i in range(3):
+        v = {}
+        for k in (-2, -1, 1, 2):
+            Lp = list(L)
+            Lp[i] += k * h
+            mm = ps.ModelAB(3, cfg["shape"], mk(Lp), cfg["Ms"], cfg["chiN"], lam=cfg["lam"])
+            mm.set_fields(wA, wB)
+            mm.forward()
+            v[k] = -np.log(mm.Q())
+            del mm
+        fd = (v[-2] - 8 * v[-1] + 8 * v[1] - v[2]) / (12 * h)
+        err_s = max(err_s, abs(fd - st[i]))
+    dA, dB = rng.standard_normal(cfg["shape"]), rng.standard_normal(cfg["shape"])
+    f = {}
+    for k in (-2, -1, 1, 2):
+        m.set_fields(wA + k * h * dA, wB + k * h * dB)
+        m.forward()
+        f[k] = float(((m.get("phiA") - tgt) ** 2).sum())
+    fd = (f[-2] - 8 * f[-1] + 8 * f[1] - f[2]) / (12 * h)
+    an = float((gA * dA).sum() + (gB * dB).sum())
+    m.set_fields(wA, wB)
+    Ns = sum(cfg["Ms"]) - 2
+    M = int(np.prod(cfg["shape"]))
+    return {"config": "C4 48^3 orthorhombic (3.8, 4.0, 4.2), Ms %s, %d Anderson iterations (residual %.1e)"
+                      % (list(cfg["Ms"]), iters, res),
+            "stress": list(st), "stress_ms": t_stress * 1e3, "loss_gradient_ms": t_grad * 1e3,
+            "stress_fd_abs_err_max": err_s, "stress_fd_rel_err_max": err_s / max(abs(x) for x in st),
+            "stress_checkpointed": list(m.stress(checkpoints=0)),
+            "gradient_fd_rel_err": abs(fd - an) / abs(an),
+            "fd_note": "4th-order central differences, h = 1e-4; their rounding floor is about 1e-16 |ln Q| / h",
+            "adjoint_gridpt_steps_per_s": Ns * M / t_stress,
+            "timing": "host wall clock around synchronised calls (forward map included)"}
+
+
 def run_reference(args, rank, world):
     """The reference algorithm's CPU restatement on all host threads (rank 0);
     each step is a bounded sample of the same workload."""
@@ -334,6 +402,7 @@ def main():
 
     string = string_method(ps) if rank == 0 and world == 1 else None
     batch = uneven_batch(ps) if rank == 0 and world == 1 else None
+    adj = adjoint_c4(ps) if rank == 0 and world == 1 else None
 
     cpu = None
     if rank == 0 and world == 1:
@@ -348,7 +417,7 @@ def main():
                 "config": {"workload": WORKLOAD, "grid": list(shape), "Ns": Ns, "Ms": list(cfg["Ms"]),
                            "l2_flush": "inputs > L2 (0.8 GB histories)", "parallelism": "replicas" if world > 1 else "single"},
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clk.summary(), "H_after": H, "string_method": string, "uneven_batch": batch}
+                "clocks": clk.summary(), "H_after": H, "string_method": string, "uneven_batch": batch, "adjoint": adj}
         print(json.dumps(line), flush=True)
     ranks.close()
 

@@ -193,6 +193,11 @@ int ps_model_ab_grad_w(ps_model_ab* m, const double* dL_dphiA, const double* dL_
  * reference's Brent cell search (src/scft.cc:589-609) estimates from
  * converged free energies. */
 int ps_model_ab_stress(ps_model_ab* m, double* dF_dl);
+/* The same stress computed with the forward chain kept only at checkpoints
+ * every k contour slices (k <= 0: ceil(sqrt(Ns))): the reverse sweep
+ * recomputes one segment at a time, so the chain needs (Ns/k + k) slices of M
+ * doubles instead of Ns + 1, for one extra forward pass. */
+int ps_model_ab_stress_checkpointed(ps_model_ab* m, int k, double* dF_dl);
 /* copy one array (PS_FIELD_*) to host memory */
 int ps_model_ab_get(ps_model_ab* m, int which, double* out);
 /* device address of one array (PS_FIELD_*), owned by the context */

@@ -189,10 +189,15 @@ class ModelAB:
                                             capi.dptr(gA), capi.dptr(gB)))
         return gA, gB
 
-    def stress(self):
-        """d(-ln Q)/dl for the three cell lengths at the current fields."""
+    def stress(self, checkpoints=None):
+        """d(-ln Q)/dl for the three cell lengths at the current fields.
+        checkpoints=k keeps the forward chain only every k slices (0: sqrt(Ns))
+        and recomputes it segment by segment in the reverse sweep."""
         out = np.zeros(3)
-        capi.check(lib().ps_model_ab_stress(self._h, capi.dptr(out)))
+        if checkpoints is None:
+            capi.check(lib().ps_model_ab_stress(self._h, capi.dptr(out)))
+        else:
+            capi.check(lib().ps_model_ab_stress_checkpointed(self._h, int(checkpoints), capi.dptr(out)))
         return out
 
     def get(self, name):

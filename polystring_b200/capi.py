@@ -79,6 +79,7 @@ SIGNATURES = [
     ("ps_model_ab_forward", ctypes.c_int, [_vp]),
     ("ps_model_ab_grad_w", ctypes.c_int, [_vp, _dp, _dp, ctypes.c_double, _dp, _dp]),
     ("ps_model_ab_stress", ctypes.c_int, [_vp, _dp]),
+    ("ps_model_ab_stress_checkpointed", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("ps_model_ab_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("ps_model_ab_device_ptr", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ps_model_ab_synchronize", ctypes.c_int, [_vp]),

@@ -134,7 +134,7 @@ int egrid(long M) {
 }  // namespace
 
 // One adjoint sweep of a chain (see the file comment and AdjointSweep).
-void PairChain::enqueue_adjoint(const AdjointSweep& s, cudaStream_t st) {
+void PairChain::enqueue_adjoint(AdjointSweep& s, cudaStream_t st) {
     if (scheme_ != SCHEME_RQM4) throw Error(-2, "the adjoint is provided for RQM4");
     if (plan_.naxes < 2) throw Error(-2, "the adjoint needs a 2D or 3D grid");
     const long M = M_;
@@ -143,12 +143,16 @@ void PairChain::enqueue_adjoint(const AdjointSweep& s, cudaStream_t st) {
     const LineGeom& out = plan_.ax[plan_.naxes - 1];
     const LineGeom* mid = (plan_.naxes == 3) ? &plan_.ax[1] : nullptr;
     if (half_.n < 2 * (size_t)M) half_.alloc(2 * (size_t)M);
-    // lambda[Ns]
-    lam_init_kernel<<<egrid(M), kAT, 0, st>>>(s.lam[0], M, s.pbarA, s.pbarB, s.wd[0][Ns], s.wd[1][Ns],
-                                                s.ho, s.cst_Ns);
-    PS_CUDA(cudaGetLastError());
-    int cur = 0;
-    for (int t = Ns - 1; t >= 0; t--) {
+    const int t_hi = s.t_hi > 0 ? s.t_hi : Ns, t_lo = s.t_lo;
+    int cur = s.lam_cur;
+    if (t_hi == Ns) {
+        // lambda[Ns]
+        lam_init_kernel<<<egrid(M), kAT, 0, st>>>(s.lam[0], M, s.pbarA, s.pbarB, s.wd[0][Ns], s.wd[1][Ns],
+                                                    s.ho, s.cst_Ns);
+        PS_CUDA(cudaGetLastError());
+        cur = 0;
+    }
+    for (int t = t_hi - 1; t >= t_lo; t--) {
         const int X = s.blk[t];
         StepPtrs p{};
         p.M = (double)M;
@@ -157,7 +161,7 @@ void PairChain::enqueue_adjoint(const AdjointSweep& s, cudaStream_t st) {
         p.half[0] = half_.p; p.half[1] = half_.p + M;
         p.z[0] = z_[0].c(); p.z[1] = z_[1].c(); p.z[2] = z_[2].c();
         p.L[0] = L1_.p; p.L[1] = L2_.p; p.L[2] = L2_.p;
-        p.qin[0] = s.hq + (long)t * M;
+        p.qin[0] = s.hq + (long)(t - s.hq_base) * M;
         p.qin[1] = s.lam[cur];
         p.qout[1] = s.lam[cur ^ 1];
         p.qout[0] = nullptr;
@@ -170,15 +174,15 @@ void PairChain::enqueue_adjoint(const AdjointSweep& s, cudaStream_t st) {
             p.other = s.ho + (long)(Ns - t) * M;
             p.wdA = s.wd[0][t]; p.wdB = s.wd[1][t];
         }
-        if (t > 0) {
+        if (t > t_lo) {
             const int Xn = s.blk[t - 1];
             p.chain_next = 1;
             p.nF[0] = p.nF[1] = s.eF[Xn];
             p.nH[0] = p.nH[1] = s.eH[Xn];
-            p.next_qf = s.hq + (long)(t - 1) * M;
+            p.next_qf = s.hq + (long)(t - 1 - s.hq_base) * M;
         }
         if (s.spec) { p.spec[0] = s.spec; p.spec[1] = s.spec + M; }
-        if (t == Ns - 1) launch_line_pass(MODE_FIRST_RQM4, in, p, 1, st);
+        if (t == t_hi - 1) launch_line_pass(MODE_FIRST_RQM4, in, p, 1, st);
         p.nfield = 2;
         if (mid) launch_line_pass(MODE_FWD, *mid, p, 1, st);
         launch_line_pass(MODE_OUTER, out, p, 1, st);
@@ -206,7 +210,7 @@ void PairChain::enqueue_adjoint(const AdjointSweep& s, cudaStream_t st) {
         }
         cur ^= 1;
     }
-    // lambda[0] ends in s.lam[cur]
+    s.lam_cur = cur;   // lambda[t_lo] is in s.lam[cur]
 }
 
 void PairChain::prepare_adjoint() {
@@ -344,6 +348,78 @@ void ModelAB::stress(double* dFdl) {
     PS_CUDA(cudaMemcpyAsync(dQ, scal_.p + 16, sizeof(double) * 3, cudaMemcpyDeviceToHost, st_));
     PS_CUDA(cudaStreamSynchronize(st_));
     for (int i = 0; i < 3; i++) dFdl[i] = -dQ[i] / Q;
+}
+
+void ModelAB::stress_checkpointed(int k, double* dFdl) {
+    if (!fields_set_) throw Error(-6, "fields are not set");
+    if (p_.mde != 0) throw Error(-2, "the adjoint is provided for RQM4");
+    if (k <= 0) k = (int)std::ceil(std::sqrt((double)Ns_));
+    if (k > Ns_) k = Ns_;
+    const int nseg = (Ns_ + k - 1) / k;
+    ensure_adjoint_buffers(true);
+    ck_.alloc((size_t)nseg * M_);
+    seg_.alloc((size_t)(k + 1) * M_);
+    if (zero_.n == 0) {
+        zero_.alloc(M_);
+        scratch_.alloc(M_);
+        launch_fill(zero_.p, M_, 0.0, st_);
+    }
+    // forward chain f only (lane c of the packed field carries zeros),
+    // keeping slice j k of every segment j
+    launch_fill(ck_.p, M_, 1.0, st_);
+    auto segment = [&](int j) {
+        const int t0 = j * k, n = std::min(k, Ns_ - t0);
+        PS_CUDA(cudaMemcpyAsync(seg_.p, ck_.p + (long)j * M_, sizeof(double) * M_, cudaMemcpyDeviceToDevice, st_));
+        LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_ - t0};
+        LaneFactors lc{{zero_.p, zero_.p}, {zero_.p, zero_.p}, 0};
+        chain_->enqueue(seg_.p, nullptr, 0, n, lf, lc, 0, st_, zero_.p, scratch_.p);
+        return n;
+    };
+    for (int j = 0; j < nseg; j++) {
+        const int n = segment(j);
+        if (j + 1 < nseg)
+            PS_CUDA(cudaMemcpyAsync(ck_.p + (long)(j + 1) * M_, seg_.p + (long)n * M_, sizeof(double) * M_,
+                                    cudaMemcpyDeviceToDevice, st_));
+    }
+    // Q = mean f[Ns]: the last slice of the last segment
+    const int nlast = Ns_ - (nseg - 1) * k;
+    double* dQ = scal_.p + 20;
+    launch_mean(seg_.p + (long)nlast * M_, M_, partial_.p, dQ, st_);
+    // reverse sweep, one recomputed segment at a time (the last one is still in seg_)
+    std::vector<double> zero(Ns_ + 1, 0.0);
+    std::vector<int> blk(Ns_);
+    for (int t = 0; t < Ns_; t++) blk[t] = t < LA_ ? 0 : 1;
+    AdjointSweep s{};
+    s.Ns = Ns_;
+    s.lam[0] = lam_.p; s.lam[1] = lam_.p + M_;
+    s.eF[0] = eFA_.p; s.eF[1] = eFB_.p; s.eH[0] = eHA_.p; s.eH[1] = eHB_.p;
+    s.grad[0] = gA_.p; s.grad[1] = gB_.p;
+    s.ds[0] = dsA_; s.ds[1] = dsB_;
+    s.blk = blk.data();
+    s.wd[0] = zero.data(); s.wd[1] = zero.data();
+    s.cst_Ns = 1.0 / (double)M_;
+    s.spec = reinterpret_cast<double2*>(spec_.p);
+    s.stress_partial = stress_part_.p;
+    const double PI = 3.14159265358979323846;
+    for (int i = 0; i < 3; i++) {
+        double l = p_.cell.l[i];
+        s.cl[i] = (i < p_.dim && l > 0) ? 8.0 * PI * PI / (l * l * l) : 0.0;
+    }
+    s.hq = seg_.p;
+    for (int j = nseg - 1; j >= 0; j--) {
+        const int n = (j == nseg - 1) ? nlast : segment(j);
+        s.t_lo = j * k;
+        s.t_hi = j * k + n;
+        s.hq_base = j * k;
+        chain_->enqueue_adjoint(s, st_);
+    }
+    stress_final_kernel<<<1, 32, 0, st_>>>(stress_part_.p, (long)Ns_ * kAG, 1.0 / (double)M_, scal_.p + 16);
+    PS_CUDA(cudaGetLastError());
+    double Q = 0.0, dQl[3];
+    PS_CUDA(cudaMemcpyAsync(&Q, dQ, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    PS_CUDA(cudaMemcpyAsync(dQl, scal_.p + 16, sizeof(double) * 3, cudaMemcpyDeviceToHost, st_));
+    PS_CUDA(cudaStreamSynchronize(st_));
+    for (int i = 0; i < 3; i++) dFdl[i] = -dQl[i] / Q;
 }
 
 }  // namespace ps

@@ -244,6 +244,13 @@ int ps_model_ab_grad_w(ps_model_ab* m, const double* dL_dphiA, const double* dL_
     });
 }
 
+int ps_model_ab_stress_checkpointed(ps_model_ab* m, int k, double* dF_dl) {
+    return guarded([&] {
+        if (!m || !dF_dl) throw Error(PS_ERR_INVALID, "null argument");
+        m->ctx->stress_checkpointed(k, dF_dl);
+    });
+}
+
 int ps_model_ab_stress(ps_model_ab* m, double* dF_dl) {
     return guarded([&] {
         if (!m || !dF_dl) throw Error(PS_ERR_INVALID, "null argument");

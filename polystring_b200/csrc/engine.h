@@ -84,6 +84,10 @@ struct AdjointSweep {
     double2* spec;             // 3 M spectra for the stress (nullable)
     double* stress_partial;    // Ns x 148 x 3
     double cl[3];              // 8 pi^2 / l^3 per axis (times the step's ds)
+    // steps t_hi-1 .. t_lo of the sweep (t_hi = 0: all Ns); slice t of the
+    // chain is at hq + (t - hq_base) M.  lambda[Ns] is set when t_hi = Ns;
+    // lam_cur carries the ping-pong index from one range to the next.
+    int t_lo, t_hi, hq_base, lam_cur;
 };
 
 // Work space and pass sequence for two real chains advanced together in one
@@ -101,7 +105,7 @@ public:
                  const LaneFactors& lc, long fac_bstride, cudaStream_t st, const double* c_in_fixed = nullptr,
                  double* c_out_fixed = nullptr);
     // reverse sweep of one chain for the w-gradient and the cell stress (RQM4, 2D/3D)
-    void enqueue_adjoint(const AdjointSweep& s, cudaStream_t st);
+    void enqueue_adjoint(AdjointSweep& s, cudaStream_t st);
     void prepare_adjoint();
     // choose each axis's tile height by timing whole contour steps (after set_tables*)
     void autotune(cudaStream_t st);
@@ -167,6 +171,10 @@ public:
     void forward_only();
     void grad_w(const double* phiA_bar, const double* phiB_bar, double Q_bar, double* gA, double* gB);
     void stress(double* dFdl);
+    // the same stress with the forward chain kept only at checkpoints every
+    // k slices (k <= 0: ceil(sqrt(Ns))), recomputed segment by segment during
+    // the reverse sweep; (Ns/k + k + 4) M doubles instead of (Ns + 1) M
+    void stress_checkpointed(int k, double* dFdl);
     // for BatchAB: the chain histories and factors, the post-propagator work
     // (Q, densities, field update) on a given stream, and the iteration count
     PairChain* chain() const { return chain_; }
@@ -209,6 +217,7 @@ private:
     DevBuf hwA_, hdA_, hwB_, hdB_, BA_, BB_;
     AXState* axs_ = nullptr;
     DevBuf lam_, gA_, gB_, pbA_, pbB_, spec_, stress_part_;
+    DevBuf ck_, seg_, zero_, scratch_;   // checkpointed stress
     long iter_ = 0;
     bool fields_set_ = false;
     bool forward_done_ = false;   // Q, phi of the current fields are valid (forward_only)

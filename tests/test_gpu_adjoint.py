@@ -136,3 +136,20 @@ def test_saddle_point_stress_matches_converged_free_energy(ps):
     Fm = converge(a - h).H()[0]
     fd = (Fp - Fm) / (2 * h)
     assert abs(fd - dFda) <= 1e-3 * abs(dFda), (fd, dFda)
+
+
+@pytest.mark.parametrize("dim,shape,cell,Ms", CASES)
+def test_checkpointed_stress_equals_full_history_stress(ps, dim, shape, cell, Ms):
+    """sqrt(Ns) checkpoints (and other segment lengths): the forward chain is
+    recomputed segment by segment during the reverse sweep; the stress agrees
+    with the full-history one to rounding (the recomputation runs the chain
+    without its packed partner, which changes roundings only)."""
+    c = ps.make_cell(dim, cell[0], *cell[1])
+    m = ps.ModelAB(dim, shape, c, Ms, 20.0)
+    m.set_fields(*_fields(shape, 6))
+    full = m.stress()
+    Ns = sum(Ms) - 2
+    for k in (0, 1, 5, Ns - 1, Ns):
+        ck = m.stress(checkpoints=k)
+        for i in range(dim):
+            assert abs(ck[i] - full[i]) <= 1e-10 * abs(full[i]), (k, i, ck[i], full[i])
