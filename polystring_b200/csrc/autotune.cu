@@ -104,6 +104,7 @@ void PairChain::autotune(cudaStream_t st) {
         sched[a] = plan_.ax[a].reg;
     }
     const std::array<int, 3> sched0 = sched;
+    std::string tried;   // every candidate's step time, for the log
     const float t_default = time_plan();
     float t_best = t_default;
     for (int sweep = 0; sweep < 2; sweep++) {
@@ -117,6 +118,10 @@ void PairChain::autotune(cudaStream_t st) {
                     set_tile_elems(plan_.ax[a], c);
                     plan_.ax[a].reg = r;
                     const float t = time_plan();
+                    char cbuf[64];
+                    std::snprintf(cbuf, sizeof(cbuf), " ax%d:%s/%d=%.1f", a, r == 0 ? "st" : (r == 1 ? "rg1" : "rg2"), c,
+                                  1e3 * t / nst);
+                    tried += cbuf;
                     if (t < 0.97f * t_best) {
                         t_best = t;
                         choice[a] = c;
@@ -142,6 +147,7 @@ void PairChain::autotune(cudaStream_t st) {
                   plan_.naxes > 1 ? names[sched0[1]] : "-", plan_.naxes > 2 ? names[sched0[2]] : "-",
                   1e3 * t_default / nst);
     std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_log += "  tried (axis:schedule/tile=us per step):" + tried + "\n";
     g_tune_cache[key] = {choice[0], choice[1], choice[2], sched[0], sched[1], sched[2]};
     g_tune_log += line;
 }

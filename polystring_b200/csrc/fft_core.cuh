@@ -46,6 +46,10 @@ PS_HD double div_rn(double x, double d, double r) {
     return fma(fma(-d, q, x), r, q);
 }
 
+// x / d for d = 2^k given r = 1/d (exact): one multiply, the same rounding
+// as the division; otherwise div_rn
+PS_HD double div_pow2_or_rn(double x, double d, double r, bool pow2) { return pow2 ? x * r : div_rn(x, d, r); }
+
 // sqrt(1/2) and sin(2 pi/3) rounded to double
 #define PS_SQRT1_2 0.70710678118654752440
 #define PS_SIN60 0.86602540378443864676

@@ -11,6 +11,12 @@
 namespace ps {
 namespace lp {
 
+// M a power of two: x / M == x * (1 / M) exactly
+__device__ __forceinline__ bool is_pow2(double M) {
+    const long long m = (long long)M;
+    return m > 0 && (m & (m - 1)) == 0;
+}
+
 constexpr int kThreads = 256;
 constexpr int kMaxEPT = 8;   // tiles hold at most 2048 elements (make_axis_plan)
 
@@ -100,6 +106,7 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
     const int nel = N * g.T;
     const double M = p.M;
     const double rM = 1.0 / M;
+    const bool mpow2 = is_pow2(M);
 
     const long oz = bz * p.bstride_z, oq = bz * p.bstride_q, oe = bz * p.bstride_e, oL = bz * p.bstride_L;
     const long ou = bz * p.bstride_u;
@@ -174,8 +181,8 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                uf[el.goff] = div_rn(v.x * ef[el.goff], M, rM);
-                uc[el.goff] = div_rn(v.y * ec[el.goff], M, rM);
+                uf[el.goff] = div_pow2_or_rn(v.x * ef[el.goff], M, rM, mpow2);
+                uc[el.goff] = div_pow2_or_rn(v.y * ec[el.goff], M, rM, mpow2);
             }
         } else {
             // first half step finishes, second half step starts
@@ -194,8 +201,8 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
                 double a = hf[el.goff], b = hc[el.goff];
-                double qtf = div_rn(v.x * a, M, rM);
-                double qtc = div_rn(v.y * b, M, rM);
+                double qtf = div_pow2_or_rn(v.x * a, M, rM, mpow2);
+                double qtc = div_pow2_or_rn(v.y * b, M, rM, mpow2);
                 if (sf) {
                     sf[ou + el.goff] = qtf;
                     sc[ou + el.goff] = qtc;
@@ -231,8 +238,8 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
             Elem el = elem<N>(g, ta, e);
             const long i = el.goff;
             double2 v = r[el.sidx];
-            double qt2 = div_rn(v.x * hf[i], M, rM);
-            double vv = div_rn(v.y * hc[i], M, rM);
+            double qt2 = div_pow2_or_rn(v.x * hf[i], M, rM, mpow2);
+            double vv = div_pow2_or_rn(v.y * hc[i], M, rM, mpow2);
             double sq = p.u[0][ou + i], sl = p.u[1][ou + i];
             double uh = p.half[0][ou + i], vh = p.half[1][ou + i];
             double q = qv[i], lam = lv[i];
@@ -277,8 +284,8 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
         PS_ELEMS(e) {
             Elem el = elem<N>(g, ta, e);
             double2 v = r[el.sidx];
-            double qf = div_rn(v.x * hf[el.goff], M, rM);
-            double qc = div_rn(v.y * hc[el.goff], M, rM);
+            double qf = div_pow2_or_rn(v.x * hf[el.goff], M, rM, mpow2);
+            double qc = div_pow2_or_rn(v.y * hc[el.goff], M, rM, mpow2);
             if constexpr (MODE == MODE_END_RQM4) {
                 qf = div_rn(4.0 * qf - p.u[0][ou + el.goff], 3.0, 1.0 / 3.0);
                 qc = div_rn(4.0 * qc - p.u[1][ou + el.goff], 3.0, 1.0 / 3.0);
@@ -341,14 +348,14 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                of[el.goff] = div_rn(v.x * ef[el.goff], M, rM);
-                oc[el.goff] = div_rn(v.y * ec[el.goff], M, rM);
+                of[el.goff] = div_pow2_or_rn(v.x * ef[el.goff], M, rM, mpow2);
+                oc[el.goff] = div_pow2_or_rn(v.y * ec[el.goff], M, rM, mpow2);
             }
         } else {
             PS_ELEMS(e) {
                 Elem el = elem<N>(g, ta, e);
                 double2 v = r[el.sidx];
-                D[el.sidx] = make_double2(div_rn(v.x * ef[el.goff], M, rM), div_rn(v.y * ec[el.goff], M, rM));
+                D[el.sidx] = make_double2(div_pow2_or_rn(v.x * ef[el.goff], M, rM, mpow2), div_pow2_or_rn(v.y * ec[el.goff], M, rM, mpow2));
             }
             const double* hf = p.eH[0] + oe;
             const double* hc = p.eH[1] + oe;
@@ -374,7 +381,7 @@ __device__ __forceinline__ void line_pass_body(const LineGeom& g, const StepPtrs
                 PS_ELEMS(e) {
                     Elem el = elem<N>(g, ta, e);
                     double2 v = r[el.sidx];
-                    C[el.sidx] = make_double2(div_rn(v.x * hf[el.goff], M, rM), div_rn(v.y * hc[el.goff], M, rM));
+                    C[el.sidx] = make_double2(div_pow2_or_rn(v.x * hf[el.goff], M, rM, mpow2), div_pow2_or_rn(v.y * hc[el.goff], M, rM, mpow2));
                 }
             }
             __syncthreads();
@@ -441,6 +448,7 @@ __device__ __forceinline__ void line_pass_body_reg(const LineGeom& g, const Step
     }
     const double M = p.M;
     const double rM = 1.0 / M;
+    const bool mpow2 = is_pow2(M);
     const long oz = bz * p.bstride_z, oq = bz * p.bstride_q, oe = bz * p.bstride_e, oL = bz * p.bstride_L;
     const long ou = bz * p.bstride_u;
     // register m of every lane holds element t + G m of its line
@@ -507,8 +515,8 @@ __device__ __forceinline__ void line_pass_body_reg(const LineGeom& g, const Step
 #pragma unroll
                 for (int m = 0; m < E; m++) {
                     const long i = off(m);
-                    p.u[0][ou + i] = div_rn(v[m].x * ef[i], M, rM);
-                    p.u[1][ou + i] = div_rn(v[m].y * ec[i], M, rM);
+                    p.u[0][ou + i] = div_pow2_or_rn(v[m].x * ef[i], M, rM, mpow2);
+                    p.u[1][ou + i] = div_pow2_or_rn(v[m].y * ec[i], M, rM, mpow2);
                 }
             }
         } else {
@@ -520,8 +528,8 @@ __device__ __forceinline__ void line_pass_body_reg(const LineGeom& g, const Step
                 if (valid) {
                     const long i = off(m);
                     const double a = hf[i], b = hc[i];
-                    const double qtf = div_rn(v[m].x * a, M, rM);
-                    const double qtc = div_rn(v[m].y * b, M, rM);
+                    const double qtf = div_pow2_or_rn(v[m].x * a, M, rM, mpow2);
+                    const double qtc = div_pow2_or_rn(v[m].y * b, M, rM, mpow2);
                     if (p.half[0]) {
                         p.half[0][ou + i] = qtf;
                         p.half[1][ou + i] = qtc;
@@ -550,8 +558,8 @@ __device__ __forceinline__ void line_pass_body_reg(const LineGeom& g, const Step
         for (int m = 0; m < E; m++) {
             if (valid) {
                 const long i = off(m);
-                double qf = div_rn(v[m].x * hf[i], M, rM);
-                double qc = div_rn(v[m].y * hc[i], M, rM);
+                double qf = div_pow2_or_rn(v[m].x * hf[i], M, rM, mpow2);
+                double qc = div_pow2_or_rn(v[m].y * hc[i], M, rM, mpow2);
                 qf = div_rn(4.0 * qf - p.u[0][ou + i], 3.0, 1.0 / 3.0);
                 qc = div_rn(4.0 * qc - p.u[1][ou + i], 3.0, 1.0 / 3.0);
                 p.qout[0][oq + i] = qf;

@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
     const long M = G::M;
     const double Md = (double)M;
     const double rMd = 1.0 / Md;
+    const bool mpow2 = (M & (M - 1)) == 0;   // x / M == x * (1 / M) exactly
     const int nb = gridDim.x;
     const long boff = (long)blockIdx.y * a.bstride_batch;   // batch offset of per-problem arrays
     unsigned bar_target = 0;
@@ -322,8 +323,8 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                             if (G::PT % kNT == 0 || p < G::PT) {
                                 long g = s0 + p;
                                 double2 v = buf[pidx<G, LZ>(p)];
-                                uf[g] = div_rn(v.x * ef[g], Md, rMd);
-                                uc[g] = div_rn(v.y * ec[g], Md, rMd);
+                                uf[g] = div_pow2_or_rn(v.x * ef[g], Md, rMd, mpow2);
+                                uc[g] = div_pow2_or_rn(v.y * ec[g], Md, rMd, mpow2);
                             }
                         }
                         __syncthreads();
@@ -338,8 +339,8 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                                 int si = pidx<G, LZ>(p);
                                 double2 v = buf[si];
                                 double ha = hfp[g], hb = hcp[g];
-                                double qtf = div_rn(v.x * ha, Md, rMd);
-                                double qtc = div_rn(v.y * hb, Md, rMd);
+                                double qtf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
+                                double qtc = div_pow2_or_rn(v.y * hb, Md, rMd, mpow2);
                                 buf[si] = make_double2(ha * qtf, hb * qtc);
                             }
                         }
@@ -375,8 +376,8 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
                     long g = s0 + p;
                     int si = pidx<G, LZ>(p);
                     double2 v = buf[si];
-                    double qf = div_rn(v.x * hfp[g], Md, rMd);
-                    double qc = div_rn(v.y * hcp[g], Md, rMd);
+                    double qf = div_pow2_or_rn(v.x * hfp[g], Md, rMd, mpow2);
+                    double qc = div_pow2_or_rn(v.y * hcp[g], Md, rMd, mpow2);
                     qf = div_rn(4.0 * qf - uf[g], 3.0, 1.0 / 3.0);
                     qc = div_rn(4.0 * qc - uc[g], 3.0, 1.0 / 3.0);
                     if (role == 0) { of[g] = qf; oc[g] = qc; }

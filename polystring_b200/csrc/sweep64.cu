@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     const int slab = b & 63, role = b >> 6;
     const long soff = (long)slab * P64;
     const double Md = (double)M64;
-    const double rMd = 1.0 / Md;
+    const double rMd = 1.0 / Md;   // M = 2^18: multiplying by 1/M rounds exactly like dividing
     unsigned* ctr = a.bar;
     unsigned bidx = 0;
     unsigned mphase = 0;
@@ -309,14 +309,14 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 for (int k = 0; k < 8; k++) {
                     const int zi = zb + 8 * k;
                     double hf = ef[zi], hc = ec[zi];
-                    ug[soff + zi] = make_double2(div_rn(v[k].x * (hf * hf), Md, rMd), div_rn(v[k].y * (hc * hc), Md, rMd));
+                    ug[soff + zi] = make_double2((v[k].x * (hf * hf)) * rMd, (v[k].y * (hc * hc)) * rMd);
                 }
             } else {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const int zi = zb + 8 * k;
                     double hf = ef[zi], hc = ec[zi];
-                    double qf = div_rn(v[k].x * hf, Md, rMd), qc = div_rn(v[k].y * hc, Md, rMd);
+                    double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
                     v[k] = make_double2(hf * qf, hc * qc);
                 }
                 plane_forward(v, s, Z3 + soff);
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 const int zi = zb + 8 * k;
                 double hf = ef[zi], hc = ec[zi];
                 double2 u = s.u[zi];
-                double qf = div_rn(v[k].x * hf, Md, rMd), qc = div_rn(v[k].y * hc, Md, rMd);
+                double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
                 qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
                 qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
                 if (role == 0) of[zi] = qf;
