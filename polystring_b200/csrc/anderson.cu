@@ -8,10 +8,10 @@
 //
 // Per iteration:
 //   ax_prepare  d(cur) = w_target - w(cur) for A and B       (update_d)
-//   ax_dots     partial sums of d(cur) . d(find_index(j)), j = 0..nn
+//   ax_dots     partial sums of d(cur) . d(find_index(j)), j = 0..nn (4 j per CTA row)
 //   ax_solve    B shift + new row (update_B), U = UA + UB, V = VA + VB,
 //               C = U^-1 V by Gaussian elimination with partial pivoting,
-//               ramp 1 - lambda^(k+1), ring position update     (one block)
+//               ramp 1 - lambda^(k+1), ring position update     (one block, shared memory)
 //   ax_combine  W = w(cur) + sum C (w(kk) - w(cur)), D likewise,
 //               w(cur') = W + ramp D, plus the next Boltzmann factors
 #include "ps_internal.h"
@@ -52,127 +52,176 @@ __global__ void ax_prepare_kernel(AXArgs a) {
     }
 }
 
+// partial sums of d(cur) . d(find_index(j)) for j = 4 blockIdx.y .. + 3
+// (both fields); every thread visits the same points i in the same order
+// for every j, so the sums do not depend on the split over blockIdx.y
+constexpr int kJC = 4;
+
 template <int NMAX>
 __global__ void __launch_bounds__(kRedThreads) ax_dots_kernel(AXArgs a, double* partial) {
     const AXState* s = a.state;
     const int n = s->n, cur = s->cur;
     const int nn = s->k < n ? s->k : n;
     const long M = a.M;
+    const int j0 = blockIdx.y * kJC;
     const double* dcA = a.dA + (long)cur * M;
     const double* dcB = a.dB + (long)cur * M;
-    double acc[2 * NMAX];
+    double acc[2 * kJC];
 #pragma unroll
-    for (int j = 0; j < 2 * NMAX; j++) acc[j] = 0.0;
-    long kk[NMAX];
+    for (int j = 0; j < 2 * kJC; j++) acc[j] = 0.0;
+    long kk[kJC];
 #pragma unroll
-    for (int j = 0; j < NMAX; j++) kk[j] = (long)find_index(cur, n, j <= nn ? j : 0) * M;
+    for (int j = 0; j < kJC; j++) kk[j] = (long)find_index(cur, n, j0 + j <= nn ? j0 + j : 0) * M;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
         double xa = dcA[i], xb = dcB[i];
 #pragma unroll
-        for (int j = 0; j < NMAX; j++) {
-            if (j <= nn) {
+        for (int j = 0; j < kJC; j++) {
+            if (j0 + j <= nn) {
                 acc[j] += xa * a.dA[kk[j] + i];
-                acc[NMAX + j] += xb * a.dB[kk[j] + i];
+                acc[kJC + j] += xb * a.dB[kk[j] + i];
             }
         }
     }
     // block reduction
-    __shared__ double sh[2 * NMAX][kRedThreads / 32];
+    __shared__ double sh[2 * kJC][kRedThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < 2 * NMAX; j++) {
+    for (int j = 0; j < 2 * kJC; j++) {
         double v = acc[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) sh[j][warp] = v;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < 2 * NMAX; j += blockDim.x) {
+    for (int q = threadIdx.x; q < 2 * kJC; q += blockDim.x) {
+        const int j = j0 + (q % kJC);
+        if (j >= NMAX) continue;
         double t = 0.0;
-        for (int w = 0; w < kRedThreads / 32; w++) t += sh[j][w];
-        partial[(long)blockIdx.x * 2 * NMAX + j] = t;
+        for (int w = 0; w < kRedThreads / 32; w++) t += sh[q][w];
+        partial[(long)blockIdx.x * 2 * NMAX + (q < kJC ? 0 : NMAX) + j] = t;
     }
 }
 
-// Gaussian elimination with partial pivoting, identical in order to the
-// oracle's orc_solve_small.  Returns 0, or -1 on an exactly zero pivot.
-__device__ int solve_small(int n, double* A, double* b, double* C) {
-    for (int k = 0; k < n; k++) {
-        int p = k;
-        double best = fabs(A[k * n + k]);
-        for (int i = k + 1; i < n; i++) {
-            double v = fabs(A[i * n + k]);
-            if (v > best) { best = v; p = i; }
-        }
-        if (best == 0.0) return -1;
-        if (p != k) {
-            for (int j = 0; j < n; j++) { double t = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = t; }
-            double t = b[k]; b[k] = b[p]; b[p] = t;
-        }
-        double piv = A[k * n + k];
-        for (int i = k + 1; i < n; i++) {
-            double f = A[i * n + k] / piv;
-            A[i * n + k] = 0.0;
-            for (int j = k + 1; j < n; j++) A[i * n + j] -= f * A[k * n + j];
-            b[i] -= f * b[k];
-        }
-    }
-    for (int i = n - 1; i >= 0; i--) {
-        double s = b[i];
-        for (int j = i + 1; j < n; j++) s -= A[i * n + j] * C[j];
-        C[i] = s / A[i * n + i];
-    }
-    return 0;
-}
-
+// update_B, U = UA + UB, V = VA + VB and C = U^-1 V by Gaussian elimination
+// with partial pivoting, in shared memory across the block.  Every matrix
+// element gets the same operations as in the oracle's orc_solve_small (row i
+// of step k: f = A[i][k] / piv, A[i][j] -= f A[k][j]); the pivot is the first
+// row of largest |A[i][k]|; back substitution runs in order on one thread.
 template <int NMAX>
 __global__ void __launch_bounds__(kRedThreads) ax_solve_kernel(AXArgs a, const double* partial, int G) {
     AXState* s = a.state;
     const int n = s->n;
     const int N1 = n + 1;
     const int nn = s->k < n ? s->k : n;
+    const int tid = threadIdx.x, nt = blockDim.x;
     __shared__ double row[2 * NMAX];
+    __shared__ double sB[2][(NMAX + 1) * (NMAX + 1)];
+    __shared__ double U[NMAX * NMAX], V[NMAX], C[NMAX], F[NMAX];
+    __shared__ int piv_row, singular;
     // fixed-order reduction of the partial sums
-    for (int j = threadIdx.x; j < 2 * NMAX; j += blockDim.x) {
+    for (int j = tid; j < 2 * NMAX; j += nt) {
         double t = 0.0;
         for (int b = 0; b < G; b++) t += partial[(long)b * 2 * NMAX + j];
         row[j] = t / (double)a.M;
     }
+    double* BG[2] = {a.BA, a.BB};
+    for (int f = 0; f < 2; f++)
+        for (int e = tid; e < N1 * N1; e += nt) sB[f][e] = BG[f][e];
+    if (tid == 0) singular = 0;
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    double* BA = a.BA;
-    double* BB = a.BB;
-    // update_B (FieldAX.cc:321-345): shift, new row 0, symmetrise
-    for (int i = n; i >= 1; i--)
-        for (int j = n; j >= i; j--) {
-            BA[i * N1 + j] = BA[(i - 1) * N1 + (j - 1)];
-            BB[i * N1 + j] = BB[(i - 1) * N1 + (j - 1)];
+    // update_B (FieldAX.cc:321-345): shift the upper triangle down the diagonal
+    double shifted[2][((NMAX + 1) * (NMAX + 1) + kRedThreads - 1) / kRedThreads];
+    for (int f = 0; f < 2; f++) {
+        int c = 0;
+        for (int e = tid; e < N1 * N1; e += nt, c++) {
+            const int i = e / N1, j = e - i * N1;
+            shifted[f][c] = (i >= 1 && j >= i) ? sB[f][(i - 1) * N1 + (j - 1)] : sB[f][e];
         }
-    for (int j = 0; j <= nn; j++) {
-        BA[j] = row[j];
-        BB[j] = row[NMAX + j];
     }
-    for (int i = 0; i < N1; i++)
-        for (int j = i + 1; j < N1; j++) {
-            BA[j * N1 + i] = BA[i * N1 + j];
-            BB[j * N1 + i] = BB[i * N1 + j];
+    __syncthreads();
+    for (int f = 0; f < 2; f++) {
+        int c = 0;
+        for (int e = tid; e < N1 * N1; e += nt, c++) sB[f][e] = shifted[f][c];
+    }
+    __syncthreads();
+    for (int j = tid; j <= nn; j += nt) {   // new row 0
+        sB[0][j] = row[j];
+        sB[1][j] = row[NMAX + j];
+    }
+    __syncthreads();
+    for (int f = 0; f < 2; f++)             // symmetrise
+        for (int e = tid; e < N1 * N1; e += nt) {
+            const int i = e / N1, j = e - i * N1;
+            if (j < i) sB[f][e] = sB[f][j * N1 + i];
         }
+    __syncthreads();
+    for (int f = 0; f < 2; f++)
+        for (int e = tid; e < N1 * N1; e += nt) BG[f][e] = sB[f][e];
     // U = UA + UB, V = VA + VB (FieldAX.cc:352-381)
-    double U[NMAX * NMAX], V[NMAX], C[NMAX];
-    for (int i = 0; i < nn; i++) {
-        for (int j = 0; j < nn; j++) {
-            double ua = BA[0] - BA[(i + 1) * N1] - BA[j + 1] + BA[(i + 1) * N1 + (j + 1)];
-            double ub = BB[0] - BB[(i + 1) * N1] - BB[j + 1] + BB[(i + 1) * N1 + (j + 1)];
-            U[i * nn + j] = 0.0 + ua + ub;
-        }
-        V[i] = 0.0 + (BA[0] - BA[(i + 1) * N1]) + (BB[0] - BB[(i + 1) * N1]);
+    const double* BA = sB[0];
+    const double* BB = sB[1];
+    for (int e = tid; e < nn * nn; e += nt) {
+        const int i = e / nn, j = e - i * nn;
+        double ua = BA[0] - BA[(i + 1) * N1] - BA[j + 1] + BA[(i + 1) * N1 + (j + 1)];
+        double ub = BB[0] - BB[(i + 1) * N1] - BB[j + 1] + BB[(i + 1) * N1 + (j + 1)];
+        U[e] = 0.0 + ua + ub;
     }
+    for (int i = tid; i < nn; i += nt) V[i] = 0.0 + (BA[0] - BA[(i + 1) * N1]) + (BB[0] - BB[(i + 1) * N1]);
+    __syncthreads();
+    for (int k = 0; k < nn; k++) {
+        if (tid == 0) {
+            int p = k;
+            double best = fabs(U[k * nn + k]);
+            for (int i = k + 1; i < nn; i++) {
+                const double v = fabs(U[i * nn + k]);
+                if (v > best) { best = v; p = i; }
+            }
+            piv_row = p;
+            if (best == 0.0) singular = 1;
+        }
+        __syncthreads();
+        if (singular) break;
+        const int p = piv_row;
+        if (p != k) {
+            for (int j = tid; j < nn; j += nt) {
+                const double t = U[k * nn + j];
+                U[k * nn + j] = U[p * nn + j];
+                U[p * nn + j] = t;
+            }
+            if (tid == 0) {
+                const double t = V[k];
+                V[k] = V[p];
+                V[p] = t;
+            }
+        }
+        __syncthreads();
+        const double pv = U[k * nn + k];
+        for (int i = k + 1 + tid; i < nn; i += nt) F[i] = U[i * nn + k] / pv;
+        __syncthreads();
+        const int w = nn - k - 1;           // columns k+1 .. nn-1 of rows k+1 .. nn-1
+        for (int e = tid; e < w * w; e += nt) {
+            const int i = k + 1 + e / w, j = k + 1 + e % w;
+            U[i * nn + j] -= F[i] * U[k * nn + j];
+        }
+        for (int i = k + 1 + tid; i < nn; i += nt) {
+            U[i * nn + k] = 0.0;
+            V[i] -= F[i] * V[k];
+        }
+        __syncthreads();
+    }
+    if (tid != 0) return;
     int nc = 0;
     if (nn > 0) {
-        if (solve_small(nn, U, V, C) != 0) {
+        if (singular) {
             s->status |= 1;
             for (int i = 0; i < nn; i++) C[i] = 0.0;
+        } else {
+            for (int i = nn - 1; i >= 0; i--) {
+                double t = V[i];
+                for (int j = i + 1; j < nn; j++) t -= U[i * nn + j] * C[j];
+                C[i] = t / U[i * nn + i];
+            }
         }
         nc = nn;
     }
@@ -251,15 +300,15 @@ void launch_anderson(const AXArgs& a, double* partial, cudaStream_t st) {
     PS_CUDA(cudaGetLastError());
     switch (nmax) {
     case 8:
-        ax_dots_kernel<8><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_dots_kernel<8><<<dim3(kRedBlocks, (8 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
         ax_solve_kernel<8><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
         break;
     case 16:
-        ax_dots_kernel<16><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_dots_kernel<16><<<dim3(kRedBlocks, (16 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
         ax_solve_kernel<16><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
         break;
     default:
-        ax_dots_kernel<32><<<kRedBlocks, kRedThreads, 0, st>>>(a, partial);
+        ax_dots_kernel<32><<<dim3(kRedBlocks, (32 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
         ax_solve_kernel<32><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
         break;
     }

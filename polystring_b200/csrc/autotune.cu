@@ -109,8 +109,12 @@ void PairChain::autotune(cudaStream_t st) {
     float t_best = t_default;
     for (int sweep = 0; sweep < 2; sweep++) {
         for (int a = 0; a < plan_.naxes; a++) {
-            const bool regok = reg_lines_per_cta(plan_.ax[a].N) > 0;
+            // a schedule forced by PS_B200_REG_FFT is kept; only tiles are tuned then
+            const char* rf = std::getenv("PS_B200_REG_FFT");
+            const bool forced = rf && rf[0] >= '0' && rf[0] <= '2';
+            const bool regok = reg_lines_per_cta(plan_.ax[a].N) > 0 && !forced;
             for (int r = 0; r <= (regok ? 2 : 0); r++) {
+                if (!regok && r != sched[a]) continue;
                 for (int c : cand) {
                     if (r > 0 && c != choice[a]) continue;          // the tile matters to Stockham only
                     if (r == sched[a] && c == choice[a]) continue;
