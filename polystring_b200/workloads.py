@@ -113,3 +113,38 @@ def string_images(m=40, shape=(128, 128, 1), L=8.0, seed=2024):
     wa = np.stack([e0A + i / (m - 1) * (e1A - e0A) for i in range(m)])
     wb = np.stack([e0B + i / (m - 1) * (e1B - e0B) for i in range(m)])
     return wa, wb
+
+
+def run_once(name):
+    """One pass of a case through the library, for profilers and smoke runs:
+    'string' (C3: 40 images of 128^2, one string iteration with one SCFT
+    iteration per image), 'batch' (nine C5 solves, one batch iteration),
+    'adjoint' (48^3 C4 shape, one stress evaluation)."""
+    import polystring_b200 as ps
+    if name == "string":
+        g = ps.StringAB(40, 2, (128, 128, 1), ps.make_cell(2, "SQUARE", 8.0), ms_from(0.35, 128), 18.0, max_iter=1)
+        wa, wb = string_images(m=40)
+        g.set_images(wa, wb)
+        g.iterate(1)
+        g.synchronize()
+        return g.H()
+    if name == "batch":
+        specs = uneven_solves(9)
+        b = ps.BatchAB([dict(dim=3, shape=s["shape"], cell=ps.make_cell(3, "CUBIC", s["cell"][1][0]), Ms=s["Ms"],
+                             chiN=s["chiN"], lam=s["lam"], scft="Anderson", n_anderson=10) for s in specs])
+        for k, s in enumerate(specs):
+            b.set_fields(k, s["wA"], s["wB"])
+        b.update(1)
+        b.synchronize()
+        return [b.H(k)[0] for k in range(len(specs))]
+    if name == "adjoint":
+        c = config("C4")
+        m = ps.ModelAB(3, c["shape"], ps.make_cell(3, "ORTHORHOMBIC", *c["cell"][1]), c["Ms"], c["chiN"])
+        m.set_fields(c["wA"], c["wB"])
+        return m.stress()
+    raise KeyError(name)
+
+
+if __name__ == "__main__":
+    import sys
+    print(run_once(sys.argv[1] if len(sys.argv) > 1 else "string"))
