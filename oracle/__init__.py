@@ -28,7 +28,7 @@ LAMELLAR, SQUARE, RECTANGULAR, HEXAGONAL2, OBLIQUE = 0, 1, 2, 3, 4
 CUBIC, TETRAGONAL, ORTHORHOMBIC, HEXAGONAL3, TRIGONAL, MONOCLINIC, TRICLINIC = 5, 6, 7, 8, 9, 10, 11
 # contour rules
 TRAPEZOID, SIMPSON, QUAD4_CLOSED, QUAD4_OPEN, QUAD4_SEMIOPEN_LEFT, QUAD4_SEMIOPEN_RIGHT = range(6)
-RQM4, OS2 = 0, 1
+RQM4, OS2, ETDRK4 = 0, 1, 2
 EM, ANDERSON = 0, 1
 
 
@@ -63,6 +63,8 @@ def lib():
         L.orc_rqm4_create.restype = vp
         L.orc_os2_create.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         L.orc_os2_create.restype = vp
+        L.orc_etdrk4_create.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.orc_etdrk4_create.restype = vp
         L.orc_updater_destroy.argtypes = [vp]
         L.orc_updater_solve.argtypes = [vp, dp, dp, ctypes.c_int]
         L.orc_mean.argtypes = [dp, ctypes.c_size_t]
@@ -155,14 +157,17 @@ def k_laplacian(g, shape, ds):
 
 
 class Updater:
-    """RQM4 (scheme 'RQM4', table = -k^2) or OS2 (scheme 'OS2', table = exp(-ds q^2))."""
+    """RQM4 (scheme 'RQM4', table = -k^2), OS2 (scheme 'OS2', table = exp(-ds q^2))
+    or ETDRK4 (scheme 'ETDRK4', table = -k^2, contour points Mc)."""
 
-    def __init__(self, scheme, table, shape, ds):
+    def __init__(self, scheme, table, shape, ds, Mc=32):
         t = _f64(table)
         self.shape = tuple(shape)
         self.M = int(np.prod(shape))
         if scheme == "RQM4":
             self.h = lib().orc_rqm4_create(_p(t), *self.shape, ds)
+        elif scheme == "ETDRK4":
+            self.h = lib().orc_etdrk4_create(_p(t), *self.shape, ds, Mc)
         else:
             self.h = lib().orc_os2_create(_p(t), *self.shape, ds)
 
@@ -235,7 +240,7 @@ class ModelAB:
             self._lapB = np.zeros(1)
         self.params = _ABParams(
             dim, shape[0], shape[1], shape[2], sA, sB, chiN, lam[0], lam[1], lam[2],
-            RQM4 if mde == "RQM4" else OS2, ANDERSON if scft == "Anderson" else EM,
+            {"RQM4": RQM4, "OS2": OS2, "ETDRK4": ETDRK4}[mde], ANDERSON if scft == "Anderson" else EM,
             n_anderson, 1 if compressible else 0, 1 if contour == "Simpson" else 0,
             _p(self._k2), _p(self._lapA), _p(self._lapB))
         self.h = None

@@ -78,3 +78,31 @@ def density(c, q, qc, ds, cc):
     for s in range(n + 1):
         acc += c[s] * (q[s] * qc[n - s])
     return acc * (cc * ds)
+
+
+def etdrk4_solve(w, qs, k2, ds, Mc=32):
+    """Etdrk4_PBC::solve (src/Etdrk4_PBC.cc:110-184) with the contour
+    coefficients of init_coefficient (:43-99), numpy.fft: the spectrum v of q
+    is carried from step to step."""
+    L = k2.astype(complex)
+    r = np.exp(1j * np.pi * (np.arange(Mc) + 0.5) / Mc)
+    x = ds * L[..., None] + r
+    ex = np.exp(x)
+    Q = ds * np.real(np.mean((np.exp(x / 2.0) - 1.0) / x, -1))
+    f1 = ds * np.real(np.mean((ex * (x * x - 3.0 * x + 4.0) - x - 4.0) / x ** 3, -1))
+    f2 = ds * np.real(np.mean((ex * (x - 2.0) + x + 2.0) / x ** 3, -1))
+    f3 = ds * np.real(np.mean((ex * (4.0 - x) - x * x - 3.0 * x - 4.0) / x ** 3, -1))
+    E, E2 = np.exp(ds * k2), np.exp(ds * k2 / 2.0)
+    F, IF = np.fft.fftn, np.fft.ifftn
+    v = F(qs[0])
+    for s in range(qs.shape[0] - 1):
+        Nv = F(-w * qs[s])
+        a = E2 * v + Q * Nv
+        Na = F(-w * np.real(IF(a)))
+        b = E2 * v + Q * Na
+        Nb = F(-w * np.real(IF(b)))
+        c = E2 * a + Q * (2.0 * Nb - Nv)
+        Nc = F(-w * np.real(IF(c)))
+        v = E * v + f1 * Nv + 2.0 * f2 * (Na + Nb) + f3 * Nc
+        qs[s + 1] = np.real(IF(v))
+    return qs

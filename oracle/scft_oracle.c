@@ -14,6 +14,8 @@
  *                   :368-418 (calc_k2_orthogonal, returns -k^2)
  *   RQM4            src/RQM4.cc:9-16 (tables), :41-93 (solve)
  *   OS2             src/PseudoSpectral.cc:190-195, :226-261
+ *   ETDRK4          src/Etdrk4_PBC.cc:14-24 (tables), :43-99 (contour
+ *                   coefficients), :110-184 (solve, carried spectrum)
  *   Propagator      src/Propagator.cc:85-93 (Q = mean of a slice)
  *   densities       src/Density.cc:107-121 (trapezoid), src/Simpson.cc:14-45,
  *                   src/Quadrature4.cc:17-197
@@ -37,6 +39,7 @@
  * Gaussian elimination with partial pivoting; the same algorithm, in the
  * same operation order, runs in the CUDA product.
  */
+#include <complex.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -371,12 +374,13 @@ void orc_k_laplacian(const double *g, int Na, int Nb, int Nc, double ds, double 
 /* Propagator updaters                                                       */
 /* ------------------------------------------------------------------------ */
 typedef struct {
-    int scheme;           /* 0 = RQM4, 1 = OS2 */
+    int scheme;           /* 0 = RQM4, 1 = OS2, 2 = ETDRK4 */
     int Lx, Ly, Lz;
     size_t M;
     double ds;
-    double *lap;          /* RQM4: exp(ds * k2); OS2: exp(-ds q^2) */
-    double *lap2;         /* RQM4: exp(0.5 ds k2) */
+    double *lap;          /* RQM4: exp(ds * k2); OS2: exp(-ds q^2); ETDRK4: E = exp(ds k2) */
+    double *lap2;         /* RQM4: exp(0.5 ds k2); ETDRK4: E2 = exp(ds k2 / 2) */
+    double *eq, *f1, *f2, *f3;   /* ETDRK4 contour coefficients Q, f1, f2, f3 */
     fft_plan3d *plan;
     cpx *buf;
 } orc_updater;
@@ -409,9 +413,113 @@ orc_updater *orc_os2_create(const double *lap, int Lx, int Ly, int Lz, double ds
     return u;
 }
 
+/* Etdrk4_PBC(uc, Lx, Ly, Lz, ds, Mc) (Etdrk4_PBC.cc:14-24, :43-99): L = -k^2
+ * (calc_k2_orthogonal), E = exp(ds L), E2 = exp(ds L / 2), and Q, f1, f2, f3
+ * as ds times the mean over Mc points r = exp(i pi (j + 1/2) / Mc) of the
+ * Kassam-Trefethen expressions at x = ds L + r:
+ *   Q  = (e^{x/2} - 1) / x,            f1 = (e^x (x^2 - 3x + 4) - x - 4) / x^3,
+ *   f2 = (e^x (x - 2) + x + 2) / x^3,  f3 = (e^x (4 - x) - x^2 - 3x - 4) / x^3 */
+orc_updater *orc_etdrk4_create(const double *k2, int Lx, int Ly, int Lz, double ds, int Mc) {
+    orc_updater *u = (orc_updater *)calloc(1, sizeof(orc_updater));
+    u->scheme = 2; u->Lx = Lx; u->Ly = Ly; u->Lz = Lz;
+    u->M = (size_t)Lx * Ly * Lz; u->ds = ds;
+    size_t M = u->M;
+    u->lap = (double *)malloc(sizeof(double) * M);
+    u->lap2 = (double *)malloc(sizeof(double) * M);
+    u->eq = (double *)malloc(sizeof(double) * M);
+    u->f1 = (double *)malloc(sizeof(double) * M);
+    u->f2 = (double *)malloc(sizeof(double) * M);
+    u->f3 = (double *)malloc(sizeof(double) * M);
+    const double PI = 3.14159265358979323846;
+    for (size_t m = 0; m < M; m++) {
+        const double L = k2[m];
+        u->lap[m] = exp(ds * L);
+        u->lap2[m] = exp(ds * L / 2.0);
+        double sq = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        for (int j = 0; j < Mc; j++) {
+            double complex r = cexp(I * (PI * (j + 0.5) / Mc));
+            double complex x = ds * L + r;
+            double complex ex = cexp(x), x2 = x * x, x3 = x2 * x;
+            sq += creal((cexp(x / 2.0) - 1.0) / x);
+            s1 += creal((ex * (x2 - 3.0 * x + 4.0) - x - 4.0) / x3);
+            s2 += creal((ex * (x - 2.0) + x + 2.0) / x3);
+            s3 += creal((ex * (4.0 - x) - x2 - 3.0 * x - 4.0) / x3);
+        }
+        u->eq[m] = ds * (sq / Mc);
+        u->f1[m] = ds * (s1 / Mc);
+        u->f2[m] = ds * (s2 / Mc);
+        u->f3[m] = ds * (s3 / Mc);
+    }
+    u->plan = plan3d_create(Lx, Ly, Lz);
+    u->buf = (cpx *)malloc(sizeof(cpx) * M);
+    return u;
+}
+
 void orc_updater_destroy(orc_updater *u) {
     if (!u) return;
-    free(u->lap); free(u->lap2); plan3d_destroy(u->plan); free(u->buf); free(u);
+    free(u->lap); free(u->lap2); free(u->eq); free(u->f1); free(u->f2); free(u->f3);
+    plan3d_destroy(u->plan); free(u->buf); free(u);
+}
+
+/* N(x) = F[-w x] with x = Re(b) / M taken from an inverse transform in b
+ * (inv != 0) or x = the real slice q (inv == 0) */
+static void etd_nonlin(orc_updater *u, const double *w, const cpx *b, const double *q, int inv, cpx *out) {
+    size_t M = u->M;
+    double rM = (double)M;
+    for (size_t m = 0; m < M; m++) {
+        double x = inv ? b[m].re / rM : q[m];
+        out[m].re = -w[m] * x;
+        out[m].im = 0.0;
+    }
+    fft3d_exec(u->plan, out, -1);
+}
+
+/* Etdrk4_PBC::solve (Etdrk4_PBC.cc:110-184), Cox-Matthews: the spectrum v of
+ * q is carried from step to step; each step takes four forward and four
+ * inverse transforms. */
+static int etdrk4_solve(orc_updater *u, const double *w, double *qs, int len) {
+    size_t M = u->M;
+    double rM = (double)M;
+    cpx *v = (cpx *)malloc(sizeof(cpx) * M), *Nv = (cpx *)malloc(sizeof(cpx) * M);
+    cpx *a = (cpx *)malloc(sizeof(cpx) * M), *Na = (cpx *)malloc(sizeof(cpx) * M);
+    cpx *Nb = (cpx *)malloc(sizeof(cpx) * M), *Nc = (cpx *)malloc(sizeof(cpx) * M);
+    cpx *t = u->buf;
+    for (size_t m = 0; m < M; m++) { v[m].re = qs[m]; v[m].im = 0.0; }
+    fft3d_exec(u->plan, v, -1);
+    for (int s = 0; s < len - 1; s++) {
+        const double *q1 = qs + (size_t)s * M;
+        double *q2 = qs + (size_t)(s + 1) * M;
+        etd_nonlin(u, w, NULL, q1, 0, Nv);
+        for (size_t m = 0; m < M; m++) {      /* a = E2 v + Q Nv */
+            a[m].re = u->lap2[m] * v[m].re + u->eq[m] * Nv[m].re;
+            a[m].im = u->lap2[m] * v[m].im + u->eq[m] * Nv[m].im;
+            t[m] = a[m];
+        }
+        fft3d_exec(u->plan, t, +1);
+        etd_nonlin(u, w, t, NULL, 1, Na);
+        for (size_t m = 0; m < M; m++) {      /* b = E2 v + Q Na */
+            t[m].re = u->lap2[m] * v[m].re + u->eq[m] * Na[m].re;
+            t[m].im = u->lap2[m] * v[m].im + u->eq[m] * Na[m].im;
+        }
+        fft3d_exec(u->plan, t, +1);
+        etd_nonlin(u, w, t, NULL, 1, Nb);
+        for (size_t m = 0; m < M; m++) {      /* c = E2 a + Q (2 Nb - Nv) */
+            t[m].re = u->lap2[m] * a[m].re + u->eq[m] * (2.0 * Nb[m].re - Nv[m].re);
+            t[m].im = u->lap2[m] * a[m].im + u->eq[m] * (2.0 * Nb[m].im - Nv[m].im);
+        }
+        fft3d_exec(u->plan, t, +1);
+        etd_nonlin(u, w, t, NULL, 1, Nc);
+        for (size_t m = 0; m < M; m++) {      /* v = E v + f1 Nv + 2 f2 (Na + Nb) + f3 Nc */
+            double c2 = 2.0 * u->f2[m];
+            v[m].re = u->lap[m] * v[m].re + u->f1[m] * Nv[m].re + c2 * (Na[m].re + Nb[m].re) + u->f3[m] * Nc[m].re;
+            v[m].im = u->lap[m] * v[m].im + u->f1[m] * Nv[m].im + c2 * (Na[m].im + Nb[m].im) + u->f3[m] * Nc[m].im;
+            t[m] = v[m];
+        }
+        fft3d_exec(u->plan, t, +1);
+        for (size_t m = 0; m < M; m++) q2[m] = t[m].re / rM;
+    }
+    free(v); free(Nv); free(a); free(Na); free(Nb); free(Nc);
+    return 0;
 }
 
 /* one split-step e^{-w h/2} F^-1[ L F[e^{-w h/2} q] ] / M  (RQM4.cc:71-75) */
@@ -430,6 +538,7 @@ static void split_step(orc_updater *u, const double *e, const double *L,
 /* RQM4::solve (RQM4.cc:41-93) / PseudoSpectral::solve (PseudoSpectral.cc:226-261).
  * qs holds len slices of M; qs[0] is the head on entry. */
 int orc_updater_solve(orc_updater *u, const double *w, double *qs, int len) {
+    if (u->scheme == 2) return etdrk4_solve(u, w, qs, len);
     size_t M = u->M;
     double ds = u->ds;
     double *expq = (double *)malloc(sizeof(double) * M);
@@ -676,7 +785,7 @@ typedef struct {
     int sA, sB;
     double chiN;
     double lamA, lamB, lamYita;
-    int mde;              /* 0 = RQM4, 1 = OS2 */
+    int mde;              /* 0 = RQM4, 1 = OS2, 2 = ETDRK4 */
     int scft;             /* 0 = EM, 1 = Anderson */
     int n_anderson;
     int compressible;
@@ -724,6 +833,10 @@ orc_model_ab *orc_model_ab_create(const orc_ab_params *p, const double *wA0, con
     if (p->mde == 0) {
         m->upA = orc_rqm4_create(p->k2, p->Lx, p->Ly, p->Lz, m->dsA);
         m->upB = orc_rqm4_create(p->k2, p->Lx, p->Ly, p->Lz, m->dsB);
+    } else if (p->mde == 2) {
+        /* the Propagator's default Etdrk4_PBC (Propagator.cc:115), M = 32 */
+        m->upA = orc_etdrk4_create(p->k2, p->Lx, p->Ly, p->Lz, m->dsA, 32);
+        m->upB = orc_etdrk4_create(p->k2, p->Lx, p->Ly, p->Lz, m->dsB, 32);
     } else {
         m->upA = orc_os2_create(p->lapA, p->Lx, p->Ly, p->Lz, m->dsA);
         m->upB = orc_os2_create(p->lapB, p->Lx, p->Ly, p->Lz, m->dsB);

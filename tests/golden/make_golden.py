@@ -11,7 +11,8 @@ PolyOrder snapshot bundled in the reference):
   those example runs (Grid gridInitType = File).
 * {1D,2D}/param.ini: the example config files, copied unchanged to
   lam1d_param.ini and lam2d_param.ini.
-* {1D,2D}/cell_opt_{rqm4,rqm4_anderson,os2,os2_anderson}.mat: the (a, F)
+* {1D,2D}/cell_opt_{rqm4,rqm4_anderson,os2,os2_anderson}.mat and
+  1D/cell_opt_{etdrk4,etdrk4_anderson}.mat: the (a, F)
   pairs written by scft::save_cell (src/scft.cc:589-609) during the Brent
   cell optimisation.  Every entry is a converged SCFT free energy H at cell
   size a (1D: thresh_residual 1e-8; 2D: 1e-6), with Ms = [51, 51],
@@ -44,6 +45,10 @@ def main(ref_root="/root/reference"):
             key = "%s_%s" % (dim.lower(), tag)
             out[key + "_a"] = np.asarray(d["a"], dtype=np.float64).ravel()
             out[key + "_F"] = np.asarray(d["F"], dtype=np.float64).ravel()
+    for tag in ("etdrk4", "etdrk4_anderson"):   # ETDRK4 traces exist for 1D only
+        d = scipy.io.loadmat(io.BytesIO(z.read(base + "1D/cell_opt_%s.mat" % tag)))
+        out["1d_%s_a" % tag] = np.asarray(d["a"], dtype=np.float64).ravel()
+        out["1d_%s_F" % tag] = np.asarray(d["F"], dtype=np.float64).ravel()
     here = os.path.dirname(os.path.abspath(__file__))
     # the example config files themselves, unchanged (inputs of the driver test)
     for dim in ("1D", "2D"):
