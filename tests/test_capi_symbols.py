@@ -73,3 +73,29 @@ def test_invalid_arguments_rejected_before_any_device_work(lib):
     # null output handle
     rc = lib.ps_updater_create(0, ctypes.byref(cell), 32, 32, 1, 0.01, None)
     assert rc == capi.PS_ERR_INVALID
+
+
+def test_newer_entry_points_check_arguments_first(lib):
+    """Batch, adjoint, checkpointed stress and the no-allocation density
+    reject bad arguments with a status before any device work."""
+    import polystring_b200 as ps
+    from polystring_b200 import capi
+    h = ctypes.c_void_p()
+    out = (ctypes.c_double * 3)()
+    assert lib.ps_batch_ab_create(None, 2, ctypes.byref(h)) == capi.PS_ERR_INVALID
+    p = ps._params(2, (32, 32, 1), ps.make_cell(2, "SQUARE", 4.0), (21, 31), 20.0)
+    assert lib.ps_batch_ab_create(ctypes.byref(p), 0, ctypes.byref(h)) == capi.PS_ERR_INVALID
+    assert lib.ps_batch_ab_update(None, 1) == capi.PS_ERR_INVALID
+    assert lib.ps_batch_ab_H(None, 0, out, out, out) == capi.PS_ERR_INVALID
+    assert lib.ps_model_ab_stress(None, out) == capi.PS_ERR_INVALID
+    assert lib.ps_model_ab_stress_checkpointed(None, 0, out) == capi.PS_ERR_INVALID
+    assert lib.ps_model_ab_forward(None) == capi.PS_ERR_INVALID
+    assert lib.ps_model_ab_grad_w(None, out, out, 0.0, out, out) == capi.PS_ERR_INVALID
+    # the no-allocation density: size limit and rule preconditions, pointers never touched
+    dummy = ctypes.c_void_p(16)
+    rc = lib.ps_density_solve_device_noalloc(0, dummy, dummy, capi.PS_DENSITY_NOALLOC_MAX_LEN + 1, 4, 0.01, 1.0,
+                                             dummy, None)
+    assert rc == capi.PS_ERR_INVALID and b"8192" in lib.ps_last_error()
+    rc = lib.ps_density_solve_device_noalloc(1, dummy, dummy, 36, 4, 0.01, 1.0, dummy, None)   # Simpson, odd n
+    assert rc == capi.PS_ERR_QUADRATURE
+    assert isinstance(lib.ps_tuning_log(), bytes)
