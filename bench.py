@@ -472,6 +472,17 @@ def main():
             "traffic": tr * units_per_step if tr else None, "peak_kind": peak_kind,
             "kernel": "propagator sweep (persistent RQM4 kernel), %d launch(es) per iteration" % m.launches_per_propagate(),
             "propagator_share_of_step": prop_s / total_s}
+    # the FP64 side of the same kernel: 6 FFTs of M points per RQM4 step at
+    # 2.5 log2(M) flops per point each, plus ~20 elementwise flops; at 64^3
+    # the FP64 floor is above the HBM floor, so report both and the fraction
+    # of the attainable (larger) floor
+    import math
+    flop = 15.0 * math.log2(M) + 20.0
+    rate = units_per_step * args.steps / prop_s
+    fp64_peak = 37.0e12        # nominal B200 FP64 (not in MEASURED_PEAKS.json)
+    roof["fp64"] = {"flop_per_gridpt_step": flop, "achieved_tflops": rate * flop / 1e12,
+                    "peak_tflops": fp64_peak / 1e12, "peak_kind": "nominal", "frac": rate * flop / fp64_peak}
+    roof["attainable_frac"] = rate * max(BYTES_PER_GRIDPT_STEP / (peak * 1e9), flop / fp64_peak)
 
     string = string_method(ps) if rank == 0 and world == 1 else None
     batch = uneven_batch(ps) if rank == 0 and world == 1 else None
