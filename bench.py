@@ -184,7 +184,7 @@ def string_method(ps, iters=10):
     return {"config": "C3 string, 40 images 128x128, Ms %s, 3 SCFT iterations per image" % list(Ms),
             "batched_string_iters_per_s": 1.0 / tb, "sequential_plain_gpu_iters_per_s": 1.0 / ts,
             "speedup_vs_sequential": ts / tb, "launches_per_string_iteration": g.launches_per_iteration(),
-            "line_pass_tiles": [l for l in ps.lib().ps_tuning_log().decode().split("\ngrid ") if "128x128x1" in l],
+            "propagator_path": [l for l in ps.lib().ps_tuning_log().decode().split("\ngrid ") if "128x128x1" in l],
             "timing": "host wall clock around synchronised replays"}
 
 

@@ -49,6 +49,11 @@ const char* tuning_log() {
     return g_tune_log.c_str();
 }
 
+void tuning_note(const char* line) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_log += line;
+}
+
 void PairChain::autotune(cudaStream_t st) {
     if (plan_.naxes < 2 || !tuning_enabled()) return;
     const TuneKey key{Lx_, Ly_, Lz_, scheme_, nbatch_, batched_tables_ ? 1 : 0};

@@ -49,6 +49,7 @@ AxisPlan make_axis_plan(int Lx, int Ly, int Lz);
 void set_tile_elems(LineGeom& g, int elems);
 // the tile choices of the autotuner so far, one line per tuned chain
 const char* tuning_log();
+void tuning_note(const char* line);   // appends one line to the tuning log
 
 enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1 };
 

@@ -15,8 +15,10 @@
 #include "engine.h"
 #include "field_kernels.h"
 #include "string_ab.h"
+#include "sweep.h"
 
 #include <cmath>
+#include <cstdlib>
 
 namespace ps {
 
@@ -195,8 +197,20 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
             L2[i] = exp(0.5 * dsA_ * k2[i]);
         }
         chain_->set_tables(L1, L2);
+        // every image's propagators in one cluster-resident sweep per SCFT
+        // iteration where the 2D grid has one (PS_B200_LINE_PASSES=1 keeps
+        // the batched line passes)
+        const char* force = getenv("PS_B200_LINE_PASSES");
+        if (cluster_sweep_supported(p.Lx, p.Ly, p.Lz) && !(force && force[0] == '1')) {
+            use_cluster_ = true;
+            cluster_sweep_prepare(p.Lx, p.Ly, p.Lz, m);
+            clL1_.alloc(M_);
+            clL2_.alloc(M_);
+            PS_CUDA(cudaMemcpy(clL1_.p, L1.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+            PS_CUDA(cudaMemcpy(clL2_.p, L2.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+        }
     }
-    chain_->autotune(st_);
+    if (!use_cluster_) chain_->autotune(st_);
     const size_t mM = (size_t)m * M_;
     hf_.alloc((size_t)(Ns_ + 1) * mM);
     hc_.alloc((size_t)(Ns_ + 1) * mM);
@@ -241,9 +255,19 @@ void StringAB::set_images(const double* wa, const double* wb, bool dev) {
 
 void StringAB::enqueue_scft_iteration() {
     const long hstride = (long)(Ns_ + 1) * M_;
-    LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
-    LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
-    chain_->enqueue(hf_.p, hc_.p, hstride, Ns_, lf, lc, M_, st_);
+    if (use_cluster_) {
+        SweepArgs a{};
+        a.hf = hf_.p; a.hc = hc_.p;
+        a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
+        a.L1 = clL1_.p; a.L2 = clL2_.p;
+        a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
+        a.bstride_batch = M_; a.bstride_hist = hstride; a.bstride_L = 0;
+        cluster_sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, m_, st_);
+    } else {
+        LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
+        LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
+        chain_->enqueue(hf_.p, hc_.p, hstride, Ns_, lf, lc, M_, st_);
+    }
     // Q of every image
     dim3 g(rgrid(M_), m_);
     breduce_partial<TailMeanF, 1><<<g, kBT, 0, st_>>>(TailMeanF{hf_.p, hstride, (long)Ns_ * M_}, M_, partial_.p);
@@ -344,7 +368,8 @@ void StringAB::get(int which, double* out, bool dev) {
 }
 
 int StringAB::launches_per_iteration() const {
-    const int scft = chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0) + 2 + 2 + 1;
+    const int prop = use_cluster_ ? 1 : chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
+    const int scft = prop + 2 + 2 + 1;
     return 2 + max_iter_ * scft + 2 + 2 + 1 + 2;
 }
 

@@ -22,6 +22,7 @@ public:
     long M() const { return M_; }
     int Ns() const { return Ns_; }
     int launches_per_iteration() const;
+    bool cluster_sweep() const { return use_cluster_; }
     cudaStream_t stream() const { return st_; }
 
 private:
@@ -36,6 +37,9 @@ private:
     cudaStream_t st_ = nullptr;
     cudaGraphExec_t giter_ = nullptr;
     DevBuf hf_, hc_, wa_, wb_, yita_, phiA_, phiB_, eFA_, eHA_, eFB_, eHB_, ends_, cA_, cB_, scal_, S_, partial_;
+    // one thread-block cluster per image for the propagators (2D grids that have one)
+    bool use_cluster_ = false;
+    DevBuf clL1_, clL2_;                 // exp(ds k2), exp(ds k2 / 2) in natural order
     long iters_ = 0;
     bool ready_ = false;
 };

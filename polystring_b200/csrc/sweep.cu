@@ -23,6 +23,7 @@
 // reports the failure.  The launch is cooperative, so all CTAs are resident.
 #include "ps_internal.h"
 #include "fft_core.cuh"
+#include "smem_line_fft.cuh"
 #include "sweep.h"
 
 namespace ps {
@@ -65,69 +66,9 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, int* err, unsigned
     return stop == 0;
 }
 
-// ---------------------------------------------------------------------------
-// in-place line FFTs with register staging
-// ---------------------------------------------------------------------------
-// Lines l = 0..NL-1 of length N; element n of line l at buf[off(l) + n*ES].
+// in-place line FFTs with register staging (smem_line_fft.cuh), kNT threads
 template <int N, int NL, int ES, class Off, int SIGN>
-struct LineFFT {
-    template <int R, int NS>
-    __device__ __forceinline__ static void pass(double2* buf, const double2* tw, const Off& off) {
-        constexpr int NB = N / R;
-        constexpr int TOTAL = NL * NB;
-        constexpr int BPT = (TOTAL + kNT - 1) / kNT;
-        double2 v[BPT][R];
-        int base[BPT], jj[BPT];
-#pragma unroll
-        for (int k = 0; k < BPT; k++) {
-            const int b = threadIdx.x + k * kNT;
-            jj[k] = -1;
-            if (TOTAL % kNT == 0 || b < TOTAL) {
-                const int l = b % NL, j = b / NL;
-                jj[k] = j;
-                base[k] = off(l);
-#pragma unroll
-                for (int r = 0; r < R; r++) v[k][r] = buf[base[k] + (j + r * NB) * ES];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < BPT; k++) {
-            if (jj[k] < 0) continue;
-            const int j = jj[k];
-            const int jm = j % NS;
-            if (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; r++) {
-                    const int m = (jm * r * (N / (NS * R))) % N;
-                    double2 w = tw[m];
-                    if (SIGN > 0) w.y = -w.y;
-                    v[k][r] = cmul(v[k][r], w);
-                }
-            }
-            Dft<R, SIGN>::run(v[k]);
-            const int idxD = (j / NS) * NS * R + jm;
-#pragma unroll
-            for (int r = 0; r < R; r++) buf[base[k] + (idxD + r * NS) * ES] = v[k][r];
-        }
-        __syncthreads();
-    }
-    __device__ __noinline__ static void run(double2* buf, const double2* tw, const Off& off) {
-        using P = Plan<N>;
-        if constexpr (P::P >= 1) pass<P::r0, 1>(buf, tw, off);
-        if constexpr (P::P >= 2) pass<P::r1, P::r0>(buf, tw, off);
-        if constexpr (P::P >= 3) pass<P::r2, P::r0 * P::r1>(buf, tw, off);
-    }
-};
-
-template <int A>
-struct OffMul {   // off(l) = l * A
-    __device__ __forceinline__ int operator()(int l) const { return l * A; }
-};
-template <int INNER, int OUTER_STRIDE>
-struct OffSplit {  // off(l) = (l / INNER) * OUTER_STRIDE + (l % INNER)
-    __device__ __forceinline__ int operator()(int l) const { return (l / INNER) * OUTER_STRIDE + (l % INNER); }
-};
+using LineFFT = SmemLineFFT<N, NL, ES, Off, SIGN, kNT>;
 
 constexpr int largest_div_le(int n, int cap) {
     int t = cap < n ? cap : n;

@@ -29,5 +29,11 @@ void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStre
 // sets kernel attributes, builds twiddles; returns the cooperative grid size
 int sweep_prepare(int Lx, int Ly, int Lz);
 void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st);
+// batches of 2D problems, one thread-block cluster per problem (cluster_sweep.cu):
+// uses hf, hc, the factors, L1, L2, LA, LB, Ns and the batch strides of SweepArgs
+bool cluster_sweep_supported(int Lx, int Ly, int Lz);
+// sets kernel attributes, builds twiddles; returns how many clusters fit at once
+int cluster_sweep_prepare(int Lx, int Ly, int Lz, int nbatch);
+void cluster_sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int nbatch, cudaStream_t st);
 
 }  // namespace ps

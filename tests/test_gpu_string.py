@@ -19,14 +19,20 @@ def _images(m, shape, L, seed):
     return workloads.string_images(m=m, shape=shape, L=L, seed=seed)
 
 
-@pytest.mark.parametrize("mde", ["RQM4", "OS2"])
-def test_string_iterations_match_oracle(ps, mde):
+@pytest.mark.parametrize("mde,path", [("RQM4", "cluster"), ("RQM4", "line_passes"), ("OS2", "line_passes")])
+def test_string_iterations_match_oracle(ps, mde, path, monkeypatch):
+    """RQM4 on 32x32 runs the cluster-resident sweep (one launch per SCFT
+    iteration: 2 + 3 * (1 + 5) + 7 launches per string iteration) unless
+    PS_B200_LINE_PASSES=1 selects the batched line passes."""
+    if path == "line_passes":
+        monkeypatch.setenv("PS_B200_LINE_PASSES", "1")
     m, shape, L, Ms, chiN = 6, (32, 32, 1), 4.0, (17, 25), 18.0
     wa, wb = _images(m, shape, L, 3)
     end_a = (wa[0].copy(), wa[-1].copy())
     end_b = (wb[0].copy(), wb[-1].copy())
     o = oracle.ModelAB(2, shape, (L, L), Ms, chiN, lam=(0.05, 0.05, 5.0), mde=mde)
     g = ps.StringAB(m, 2, shape, ps.make_cell(2, "SQUARE", L), Ms, chiN, lam=(0.05, 0.05, 5.0), mde=mde, max_iter=3)
+    assert (g.launches_per_iteration() == 27) == (path == "cluster")
     g.set_images(wa, wb)
     wa_o, wb_o = wa.copy(), wb.copy()
     for it in range(3):
@@ -63,3 +69,28 @@ def test_full_string_properties(ps):
         single.set_fields(wa[s], wb[s])
         single.update(3)
         assert abs(single.H()[0] - g2.H()[s]) < 1e-11 * abs(single.H()[0])
+
+
+@pytest.mark.parametrize("shape,L", [((64, 64, 1), 6.0), ((128, 128, 1), 8.0)])
+def test_cluster_sweep_matches_line_passes(ps, shape, L, monkeypatch):
+    """The cluster-resident sweep and the batched line passes give the same
+    string iteration (two FFT orders, so equal to rounding)."""
+    from polystring_b200 import workloads
+    m = 9
+    Ms = workloads.ms_from(0.35, 128)
+    wa, wb = workloads.string_images(m=m, shape=shape, L=L, seed=5)
+    out = {}
+    for path in ("cluster", "line_passes"):
+        if path == "line_passes":
+            monkeypatch.setenv("PS_B200_LINE_PASSES", "1")
+        g = ps.StringAB(m, 2, shape, ps.make_cell(2, "SQUARE", L), Ms, 18.0, max_iter=3)
+        assert (g.launches_per_iteration() == 27) == (path == "cluster")
+        g.set_images(wa, wb)
+        g.iterate(2)
+        out[path] = (g.H(), g.get("wa"), g.get("phiA"))
+        del g
+    Hc, wc, pc = out["cluster"]
+    Hl, wl, pl = out["line_passes"]
+    np.testing.assert_allclose(Hc, Hl, rtol=1e-12, atol=0)
+    assert np.abs(wc - wl).max() < 1e-11 * np.abs(wl).max()
+    assert np.abs(pc - pl).max() < 1e-11
