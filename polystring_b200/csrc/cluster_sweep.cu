@@ -7,7 +7,8 @@
 // packed complex work fields (lane f = forward chain in the real part, lane c
 // = complementary chain in the imaginary part, as in the line passes) fit in
 // the shared memory of C CTAs: CTA r of the cluster owns rows x in
-// [r LX/C, (r+1) LX/C) in "row layout" (y lines contiguous, pitch LY + 1).
+// [r LX/C, (r+1) LX/C) in "row layout" (y lines contiguous, pitch LY + 1,
+// y swizzled within aligned groups of 8).
 // A 2D transform is
 //
 //   y FFTs in row layout | cluster transpose | x FFTs in column layout
@@ -33,7 +34,6 @@
 
 #include "ps_internal.h"
 #include "fft_core.cuh"
-#include "smem_line_fft.cuh"
 #include "engine.h"
 #include "sweep.h"
 
@@ -43,82 +43,146 @@ namespace ps {
 
 namespace {
 
-constexpr int kCT = 256;   // threads per CTA
+constexpr int kCT = 128;   // threads per CTA (168 registers a thread at 3 CTAs per SM)
 
-template <int LX, int LY, int C>
+// The CTA's shared memory: twiddles, then field A, then field B.  Passes
+// address it by offset, so the compiler knows every such access is a shared
+// one (and cannot alias the global factor tables and histories).
+extern __shared__ double2 csm[];
+
+template <int LX, int LY, int C, int NT>
 struct CGeo {
     static constexpr int XR = LX / C;          // rows per CTA (row layout)
     static constexpr int YC = LY / C;          // columns per CTA (column layout)
     static constexpr int RP = LY + 1;          // row pitch in double2
     static constexpr int FS = XR * RP;         // one field's buffer (double2)
     static constexpr int E = XR * LY;          // points per CTA (= LX * YC)
-    static constexpr int EPT = E / kCT;        // points per thread
+    static constexpr int EPT = E / NT;         // points per thread
     static constexpr long M = (long)LX * LY;
     static_assert(LX % C == 0 && LY % C == 0, "C must divide both axes");
-    static_assert(E % kCT == 0 && E / kCT >= 1, "whole points per thread");
+    static_assert(E % NT == 0 && E / NT >= 1, "whole points per thread");
     static_assert(LX * YC == E && E <= FS, "column layout fits the row buffer");
 };
 
-// row-layout index of CTA-local point e (x_local = e / LY, y = e % LY)
-template <class G, int LY>
-__device__ __forceinline__ int ridx(int e) { return (e / LY) * G::RP + (e % LY); }
+// two radix passes per line length: r0 first (no twiddles), then r1
+template <int N> struct Plan2;
+template <> struct Plan2<32> { static constexpr int r0 = 8, r1 = 4; };
+template <> struct Plan2<64> { static constexpr int r0 = 8, r1 = 8; };
+template <> struct Plan2<128> { static constexpr int r0 = 16, r1 = 8; };
 
-// peers' row-layout points -> this CTA's column-layout points (e = x * YC + yl)
-template <class G>
-__device__ __forceinline__ void gather_rc(double2 (&v)[G::EPT], double2* fld, int r, cg::cluster_group& cl) {
-#pragma unroll
-    for (int k = 0; k < G::EPT; k++) {
-        const int e = threadIdx.x + k * kCT;
-        const int x = e / G::YC, yl = e % G::YC;
-        const double2* src = cl.map_shared_rank(fld, (unsigned)(x / G::XR));
-        v[k] = src[(x % G::XR) * G::RP + r * G::YC + yl];
-    }
-}
-template <class G>
-__device__ __forceinline__ void put_c(const double2 (&v)[G::EPT], double2* fld) {
-#pragma unroll
-    for (int k = 0; k < G::EPT; k++) fld[threadIdx.x + k * kCT] = v[k];
-}
-// peers' column-layout points -> this CTA's row-layout points
-template <class G, int LY>
-__device__ __forceinline__ void gather_cr(double2 (&v)[G::EPT], double2* fld, int r, cg::cluster_group& cl) {
-#pragma unroll
-    for (int k = 0; k < G::EPT; k++) {
-        const int e = threadIdx.x + k * kCT;
-        const int xl = e / LY, y = e % LY;
-        const double2* src = cl.map_shared_rank(fld, (unsigned)(y / G::YC));
-        v[k] = src[(r * G::XR + xl) * G::YC + (y % G::YC)];
-    }
-}
-template <class G, int LY>
-__device__ __forceinline__ void put_r(const double2 (&v)[G::EPT], double2* fld) {
-#pragma unroll
-    for (int k = 0; k < G::EPT; k++) fld[ridx<G, LY>(threadIdx.x + k * kCT)] = v[k];
+// butterfly b of a pass over NL lines with NB butterflies a line: LFAST puts
+// consecutive threads on consecutive lines, otherwise on consecutive
+// butterflies of one line (consecutive elements of the line)
+template <int NL, int NB, bool LFAST>
+__device__ __forceinline__ void bmap(int b, int& l, int& j) {
+    if (LFAST) { l = b % NL; j = b / NL; } else { j = b % NB; l = b / NB; }
 }
 
-template <int LX, int LY, int C, class PX, class PY>
+// One Stockham butterfly of N-point lines: inputs v[r] = x[j + r N/R] after
+// the twiddles of stage NS, outputs y[(j / NS) NS R + j % NS + r NS].
+template <int N, int R, int NS, int SIGN>
+__device__ __forceinline__ void butterfly(double2 (&v)[R], int j, const double2* tw) {
+    if (NS > 1) {
+        const int jm = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            double2 w = tw[(jm * r * (N / (NS * R))) % N];
+            if (SIGN > 0) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+    }
+    Dft<R, SIGN>::run(v);
+}
+template <int R, int NS>
+__device__ __forceinline__ int out_base(int j) { return (j / NS) * NS * R + j % NS; }
+
+struct NoEpi {
+    __device__ __forceinline__ double2 operator()(int, int, double2 v) const { return v; }
+};
+
+// One in-place pass over NL lines of this CTA's buffer: ad(l, n) is the index
+// of element n of line l; epi(l, n, value) gives what is stored at output n
+// (the pass's fused epilogue).  Starts and ends with the CTA synchronised.
+template <int N, int R, int NS, int SIGN, int NL, bool LFAST, class Ad, class Epi>
+__device__ __noinline__ void local_pass(int buf, int tw, Ad ad, Epi epi) {
+    constexpr int NB = N / R, TOTAL = NL * NB, BPT = (TOTAL + kCT - 1) / kCT;
+    double2 v[BPT][R];
+    int ll[BPT], jj[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        const int b = threadIdx.x + k * kCT;
+        jj[k] = -1;
+        if (TOTAL % kCT == 0 || b < TOTAL) {
+            bmap<NL, NB, LFAST>(b, ll[k], jj[k]);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[k][r] = csm[buf + ad(ll[k], jj[k] + r * NB)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        if (jj[k] < 0) continue;
+        butterfly<N, R, NS, SIGN>(v[k], jj[k], csm + tw);
+        const int o = out_base<R, NS>(jj[k]);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int n = o + r * NS;
+            csm[buf + ad(ll[k], n)] = epi(ll[k], n, v[k][r]);
+        }
+    }
+    __syncthreads();
+}
+
+// The first radix pass of the other axis fused with the cluster transpose:
+// the butterfly inputs come from the peers' buffers (src(l, n) points at
+// element n of line l there), the butterflies run in registers, a cluster
+// barrier makes sure no CTA still reads this CTA's buffer, then the outputs
+// overwrite it (ad(l, n) as in local_pass).  The caller has synchronised the
+// cluster after the peers' buffers became final.
+template <int N, int R, int SIGN, int NL, bool LFAST, class Src, class Ad>
+__device__ __noinline__ void gather_pass(int buf, Src src, Ad ad) {
+    constexpr int NB = N / R, TOTAL = NL * NB, BPT = (TOTAL + kCT - 1) / kCT;
+    double2 v[BPT][R];
+    int ll[BPT], jj[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        const int b = threadIdx.x + k * kCT;
+        jj[k] = -1;
+        if (TOTAL % kCT == 0 || b < TOTAL) {
+            bmap<NL, NB, LFAST>(b, ll[k], jj[k]);
+#pragma unroll
+            for (int r = 0; r < R; r++) v[k][r] = *src(ll[k], jj[k] + r * NB);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < BPT; k++)
+        if (jj[k] >= 0) butterfly<N, R, 1, SIGN>(v[k], jj[k], nullptr);
+    cg::this_cluster().sync();
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        if (jj[k] < 0) continue;
+        const int o = out_base<R, 1>(jj[k]);
+#pragma unroll
+        for (int r = 0; r < R; r++) csm[buf + ad(ll[k], o + r)] = v[k][r];
+    }
+}
+
+template <int LX, int LY, int C>
 __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
-    using G = CGeo<LX, LY, C>;
-    // One field at a time: an in-place pass holds all of a thread's points in
-    // registers across its barrier, 8 double2 per field at 128^2 / 8 CTAs.
-    // y lines (row layout: element y of row xl at xl * RP + y)
-    using YF = SmemLineFFT<LY, G::XR, 1, OffMul<G::RP>, -1, kCT, PY>;
-    using YI = SmemLineFFT<LY, G::XR, 1, OffMul<G::RP>, +1, kCT, PY>;
-    // x lines (column layout: element x of column yl at x * YC + yl)
-    using XF = SmemLineFFT<LX, G::YC, G::YC, OffMul<1>, -1, kCT, PX>;
-    using XI = SmemLineFFT<LX, G::YC, G::YC, OffMul<1>, +1, kCT, PX>;
+    using G = CGeo<LX, LY, C, kCT>;
+    constexpr int X0 = Plan2<LX>::r0, X1 = Plan2<LX>::r1;
+    constexpr int Y0 = Plan2<LY>::r0, Y1 = Plan2<LY>::r1;
+    // gathers: x lines (one per local column) from the peers' rows, y lines
+    // (one per local row) from the peers' columns, consecutive threads on
+    // consecutive peer addresses
 
     cg::cluster_group cl = cg::this_cluster();
-    const int r = (int)cl.block_rank();
+    const int rk = (int)cl.block_rank();
     const long img = blockIdx.x / C;
 
-    extern __shared__ double2 sm[];
-    double2* twx = sm;
-    double2* twy = twx + LX;
-    double2* A = twy + LY;
-    double2* B = A + G::FS;
-    for (int i = threadIdx.x; i < LX; i += kCT) twx[i] = a.twx[i];
-    for (int i = threadIdx.x; i < LY; i += kCT) twy[i] = a.twy[i];
+    constexpr int twx = 0, twy = LX, A = LX + LY, B = LX + LY + G::FS;   // offsets in csm
+    for (int i = threadIdx.x; i < LX; i += kCT) csm[twx + i] = a.twx[i];
+    for (int i = threadIdx.x; i < LY; i += kCT) csm[twy + i] = a.twy[i];
 
     const long M = G::M;
     const double Md = (double)M;
@@ -129,7 +193,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     double* hc = a.hc + img * a.bstride_hist;
     const double* L1 = a.L1 + img * a.bstride_L;
     const double* L2 = a.L2 + img * a.bstride_L;
-    const long g0 = (long)r * G::E;          // this CTA's rows in natural order
+    const long g0 = (long)rk * G::E;         // this CTA's rows in natural order
     auto eF = [&](int lane, int t) -> const double* {   // e^{-w ds/2} of the lane's block at step t
         int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
         return (blk == 0 ? a.eFA : a.eFB) + boff;
@@ -138,23 +202,55 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
         return (blk == 0 ? a.eHA : a.eHB) + boff;
     };
-    double2 v[G::EPT];
 
-    // k-space multiply in column layout: B by L2 (half step), A by L1 (full step)
-    auto kmul = [&](bool both) {
-#pragma unroll 4
-        for (int k = 0; k < G::EPT; k++) {
-            const int e = threadIdx.x + k * kCT;
-            const long kx = (long)(e / G::YC) * LY + r * G::YC + (e % G::YC);
-            double l2 = L2[kx];
-            double2 b = B[e];
-            B[e] = make_double2(b.x * l2, b.y * l2);
-            if (both) {
-                double l1 = L1[kx];
-                double2 c = A[e];
-                A[e] = make_double2(c.x * l1, c.y * l1);
-            }
-        }
+    // layouts: row (l = local row, n = y) and column (l = local column, n = x)
+    // (row layout: y swizzled within aligned groups of 8, n ^ ((n / 16) % 8), so
+    // that the 16 outputs of one radix-16 butterfly, 16 apart in a row, fall
+    // in different banks; the pitch LY + 1 separates the rows)
+    auto rowAd = [](int l, int n) { return l * G::RP + (n ^ ((n >> 4) & 7)); };
+    auto colAd = [](int l, int n) { return n * G::YC + l; };
+    // element n = x of local column l, from the row layout of the CTA owning x
+    auto fromRows = [&](int fld) {
+        return [fld, rk](int l, int n) -> const double2* {
+            const int y = rk * G::YC + l;
+            return cg::this_cluster().map_shared_rank(csm + fld, (unsigned)(n / G::XR)) + (n % G::XR) * G::RP +
+                   (y ^ ((y >> 4) & 7));
+        };
+    };
+    // element n = y of local row l, from the column layout of the CTA owning y
+    auto fromCols = [&](int fld) {
+        return [fld, rk](int l, int n) -> const double2* {
+            return cg::this_cluster().map_shared_rank(csm + fld, (unsigned)(n / G::YC)) + (rk * G::XR + l) * G::YC +
+                   (n % G::YC);
+        };
+    };
+    // forward y transform in row layout
+    auto fwd_y = [&](int fld) {
+        local_pass<LY, Y0, 1, -1, G::XR, true>(fld, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, -1, G::XR, false>(fld, twy, rowAd, NoEpi());
+    };
+    // x transform, k-space multiply by Lk, inverse x transform, in column layout
+    // (the first forward pass was the gather)
+    auto x_prop = [&](int fld, const double* Lk) {
+        auto kmul = [Lk, rk](int l, int n, double2 v) {
+            const double f = __ldg(Lk + (long)n * LY + rk * G::YC + l);
+            return make_double2(v.x * f, v.y * f);
+        };
+        local_pass<LX, X1, X0, -1, G::YC, true>(fld, twx, colAd, kmul);
+        local_pass<LX, X0, 1, +1, G::YC, true>(fld, twx, colAd, NoEpi());
+        local_pass<LX, X1, X0, +1, G::YC, true>(fld, twx, colAd, NoEpi());
+    };
+    // peers' rows -> first x pass -> this CTA's columns (both fields or one)
+    auto rows_to_cols = [&](bool both) {
+        cl.sync();                                   // every CTA's rows final
+        gather_pass<LX, X0, -1, G::YC, true>(B, fromRows(B), colAd);
+        if (both) gather_pass<LX, X0, -1, G::YC, true>(A, fromRows(A), colAd);
+        __syncthreads();
+    };
+    auto cols_to_rows = [&](bool both) {
+        cl.sync();                                   // every CTA's columns final
+        gather_pass<LY, Y0, +1, G::XR, false>(B, fromCols(B), rowAd);
+        if (both) gather_pass<LY, Y0, +1, G::XR, false>(A, fromCols(A), rowAd);
         __syncthreads();
     };
 
@@ -165,114 +261,74 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         for (int k = 0; k < G::EPT; k++) {
             const int e = threadIdx.x + k * kCT;
             const long g = g0 + e;
-            const int si = ridx<G, LY>(e);
+            const int si = rowAd(e / LY, e % LY);
             const double qf = hf[g], qc = hc[g];
-            A[si] = make_double2(ef[g] * qf, ec[g] * qc);
-            B[si] = make_double2(hfp[g] * qf, hcp[g] * qc);
+            csm[A + si] = make_double2(__ldg(ef + g) * qf, __ldg(ec + g) * qc);
+            csm[B + si] = make_double2(__ldg(hfp + g) * qf, __ldg(hcp + g) * qc);
         }
     }
     __syncthreads();
 
     for (int t = 0; t < a.Ns; t++) {
-        // ---- full step (A, L1) and first half step (B, L2) -------------------
-        YF::run(A, twy, OffMul<G::RP>());
-        YF::run(B, twy, OffMul<G::RP>());
-        cl.sync();                                   // rows of every CTA final
-        gather_rc<G>(v, A, r, cl);
-        cl.sync();                                   // no CTA reads A any more
-        put_c<G>(v, A);
-        gather_rc<G>(v, B, r, cl);
-        cl.sync();                                   // no CTA reads B any more
-        put_c<G>(v, B);
-        __syncthreads();
-        XF::run(A, twx, OffMul<1>());
-        XF::run(B, twx, OffMul<1>());
-        kmul(true);
-        XI::run(A, twx, OffMul<1>());
-        XI::run(B, twx, OffMul<1>());
-        cl.sync();                                   // columns of every CTA final
-        gather_cr<G, LY>(v, A, r, cl);
-        cl.sync();
-        put_r<G, LY>(v, A);
-        gather_cr<G, LY>(v, B, r, cl);
-        cl.sync();
-        put_r<G, LY>(v, B);
-        __syncthreads();
-        YI::run(A, twy, OffMul<G::RP>());
-        YI::run(B, twy, OffMul<G::RP>());
-        {
-            const double *ef = eF(0, t), *ec = eF(1, t), *hfp = eH(0, t), *hcp = eH(1, t);
-#pragma unroll 4
-            for (int k = 0; k < G::EPT; k++) {
-                const int e = threadIdx.x + k * kCT;
-                const long g = g0 + e;
-                const int si = ridx<G, LY>(e);
-                const double2 z1 = A[si];
-                A[si] = make_double2(div_pow2_or_rn(z1.x * ef[g], Md, rMd, mpow2),
-                                     div_pow2_or_rn(z1.y * ec[g], Md, rMd, mpow2));
-                const double2 z2 = B[si];
-                const double ha = hfp[g], hb = hcp[g];
-                const double qtf = div_pow2_or_rn(z2.x * ha, Md, rMd, mpow2);
-                const double qtc = div_pow2_or_rn(z2.y * hb, Md, rMd, mpow2);
-                B[si] = make_double2(ha * qtf, hb * qtc);
-            }
-        }
-        __syncthreads();
-        // ---- second half step (B, L2) -----------------------------------------
-        YF::run(B, twy, OffMul<G::RP>());
-        cl.sync();
-        gather_rc<G>(v, B, r, cl);
-        cl.sync();
-        put_c<G>(v, B);
-        __syncthreads();
-        XF::run(B, twx, OffMul<1>());
-        kmul(false);
-        XI::run(B, twx, OffMul<1>());
-        cl.sync();
-        gather_cr<G, LY>(v, B, r, cl);
-        cl.sync();
-        put_r<G, LY>(v, B);
-        __syncthreads();
-        YI::run(B, twy, OffMul<G::RP>());
-        // ---- q[t+1] = (4 qt2 - u) / 3; next step's A and B --------------------
-        {
-            const bool next = t + 1 < a.Ns;
-            const double *hfp = eH(0, t), *hcp = eH(1, t);
-            const double *nf1 = eF(0, t + 1), *nc1 = eF(1, t + 1), *nf2 = eH(0, t + 1), *nc2 = eH(1, t + 1);
-            double* of = hf + (long)(t + 1) * M;
-            double* oc = hc + (long)(t + 1) * M;
-#pragma unroll 4
-            for (int k = 0; k < G::EPT; k++) {
-                const int e = threadIdx.x + k * kCT;
-                const long g = g0 + e;
-                const int si = ridx<G, LY>(e);
-                const double2 z3 = B[si];
-                const double2 u = A[si];
-                double qf = div_pow2_or_rn(z3.x * hfp[g], Md, rMd, mpow2);
-                double qc = div_pow2_or_rn(z3.y * hcp[g], Md, rMd, mpow2);
-                qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
-                qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
-                of[g] = qf;
-                oc[g] = qc;
-                if (next) {
-                    A[si] = make_double2(nf1[g] * qf, nc1[g] * qc);
-                    B[si] = make_double2(nf2[g] * qf, nc2[g] * qc);
-                }
-            }
-        }
-        __syncthreads();
+        const double *ef = eF(0, t), *ec = eF(1, t), *hfp = eH(0, t), *hcp = eH(1, t);
+        // ---- full step (A, L1) and first half step (B, L2) ---------------------
+        fwd_y(A);
+        fwd_y(B);
+        rows_to_cols(true);
+        x_prop(A, L1);
+        x_prop(B, L2);
+        cols_to_rows(true);
+        // last inverse y pass; u = e^{-w ds/2} A / M stays in A,
+        // B <- e^{-w ds/4} (e^{-w ds/4} B / M)
+        local_pass<LY, Y1, Y0, +1, G::XR, false>(A, twy, rowAd, [=](int l, int n, double2 v) {
+            const long g = g0 + l * LY + n;
+            return make_double2(div_pow2_or_rn(v.x * __ldg(ef + g), Md, rMd, mpow2),
+                                div_pow2_or_rn(v.y * __ldg(ec + g), Md, rMd, mpow2));
+        });
+        local_pass<LY, Y1, Y0, +1, G::XR, false>(B, twy, rowAd, [=](int l, int n, double2 v) {
+            const long g = g0 + l * LY + n;
+            const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
+            const double qtf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
+            const double qtc = div_pow2_or_rn(v.y * hb, Md, rMd, mpow2);
+            return make_double2(ha * qtf, hb * qtc);
+        });
+        // ---- second half step (B, L2) -------------------------------------------
+        fwd_y(B);
+        rows_to_cols(false);
+        x_prop(B, L2);
+        cols_to_rows(false);
+        // last inverse y pass fused with q[t+1] = (4 qt2 - u) / 3, the history
+        // write and the next step's inputs A = e^{-w ds/2} q, B = e^{-w ds/4} q
+        const bool next = t + 1 < a.Ns;
+        const double *nf1 = eF(0, t + 1), *nc1 = eF(1, t + 1), *nf2 = eH(0, t + 1), *nc2 = eH(1, t + 1);
+        double* of = hf + (long)(t + 1) * M;
+        double* oc = hc + (long)(t + 1) * M;
+        local_pass<LY, Y1, Y0, +1, G::XR, false>(B, twy, rowAd, [=](int l, int n, double2 v) {
+            const long g = g0 + l * LY + n;
+            const int si = rowAd(l, n);
+            const double2 u = csm[A + si];
+            double qf = div_pow2_or_rn(v.x * __ldg(hfp + g), Md, rMd, mpow2);
+            double qc = div_pow2_or_rn(v.y * __ldg(hcp + g), Md, rMd, mpow2);
+            qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
+            qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
+            of[g] = qf;
+            oc[g] = qc;
+            if (!next) return v;
+            csm[A + si] = make_double2(__ldg(nf1 + g) * qf, __ldg(nc1 + g) * qc);
+            return make_double2(__ldg(nf2 + g) * qf, __ldg(nc2 + g) * qc);
+        });
     }
     cl.sync();   // no peer reads this CTA's shared memory after it exits
 }
 
 template <int LX, int LY, int C>
 auto kernel_of() {
-    return cluster_sweep2d_kernel<LX, LY, C, Plan<LX>, Plan<LY>>;
+    return cluster_sweep2d_kernel<LX, LY, C>;
 }
 
 template <int LX, int LY, int C>
 size_t cl_smem() {
-    using G = CGeo<LX, LY, C>;
+    using G = CGeo<LX, LY, C, kCT>;
     return sizeof(double2) * ((size_t)LX + LY + 2 * (size_t)G::FS);
 }
 
@@ -296,6 +352,8 @@ template <int LX, int LY, int C>
 int cluster_prepare_t(int nbatch) {
     auto k = kernel_of<LX, LY, C>();
     PS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cl_smem<LX, LY, C>()));
+    // the whole unified L1 as shared memory, so three CTAs fit on an SM
+    PS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = cl_config<LX, LY, C>(nbatch, nullptr, attr);
     int n = 0, per_sm = 0;
