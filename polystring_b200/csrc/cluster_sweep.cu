@@ -50,6 +50,12 @@ constexpr int kCT = 128;   // threads per CTA (168 registers a thread at 3 CTAs 
 // one (and cannot alias the global factor tables and histories).
 extern __shared__ double2 csm[];
 
+// two radix passes per line length: r0 first (no twiddles), then r1
+template <int N> struct Plan2;
+template <> struct Plan2<32> { static constexpr int r0 = 8, r1 = 4; };
+template <> struct Plan2<64> { static constexpr int r0 = 8, r1 = 8; };
+template <> struct Plan2<128> { static constexpr int r0 = 16, r1 = 8; };
+
 template <int LX, int LY, int C, int NT>
 struct CGeo {
     static constexpr int XR = LX / C;          // rows per CTA (row layout)
@@ -59,16 +65,12 @@ struct CGeo {
     static constexpr int E = XR * LY;          // points per CTA (= LX * YC)
     static constexpr int EPT = E / NT;         // points per thread
     static constexpr long M = (long)LX * LY;
+    static constexpr int TWX = (Plan2<LX>::r1 - 1) * Plan2<LX>::r0;   // stage twiddles (x passes)
+    static constexpr int TWY = (Plan2<LY>::r1 - 1) * Plan2<LY>::r0;
     static_assert(LX % C == 0 && LY % C == 0, "C must divide both axes");
     static_assert(E % NT == 0 && E / NT >= 1, "whole points per thread");
     static_assert(LX * YC == E && E <= FS, "column layout fits the row buffer");
 };
-
-// two radix passes per line length: r0 first (no twiddles), then r1
-template <int N> struct Plan2;
-template <> struct Plan2<32> { static constexpr int r0 = 8, r1 = 4; };
-template <> struct Plan2<64> { static constexpr int r0 = 8, r1 = 8; };
-template <> struct Plan2<128> { static constexpr int r0 = 16, r1 = 8; };
 
 // butterfly b of a pass over NL lines with NB butterflies a line: LFAST puts
 // consecutive threads on consecutive lines, otherwise on consecutive
@@ -79,14 +81,17 @@ __device__ __forceinline__ void bmap(int b, int& l, int& j) {
 }
 
 // One Stockham butterfly of N-point lines: inputs v[r] = x[j + r N/R] after
-// the twiddles of stage NS, outputs y[(j / NS) NS R + j % NS + r NS].
+// the twiddles of stage NS, outputs y[(j / NS) NS R + j % NS + r NS].  Only
+// the last pass of a two-pass plan (NS R = N) has twiddles, W_N^{jm r}, read
+// from the stage table tw[(r - 1) NS + jm] (consecutive jm, consecutive banks).
 template <int N, int R, int NS, int SIGN>
 __device__ __forceinline__ void butterfly(double2 (&v)[R], int j, const double2* tw) {
+    static_assert(NS == 1 || NS * R == N, "twiddles only in the last of two passes");
     if (NS > 1) {
         const int jm = j % NS;
 #pragma unroll
         for (int r = 1; r < R; r++) {
-            double2 w = tw[(jm * r * (N / (NS * R))) % N];
+            double2 w = tw[(r - 1) * NS + jm];
             if (SIGN > 0) w.y = -w.y;
             v[r] = cmul(v[r], w);
         }
@@ -157,7 +162,11 @@ __device__ __noinline__ void gather_pass(int buf, Src src, Ad ad) {
 #pragma unroll
     for (int k = 0; k < BPT; k++)
         if (jj[k] >= 0) butterfly<N, R, 1, SIGN>(v[k], jj[k], nullptr);
-    cg::this_cluster().sync();
+    // every value read from the peers is consumed above, so the reads are
+    // complete: a relaxed cluster barrier (no fence) orders them before the
+    // peers overwrite their buffers, and this CTA's before it overwrites its own
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
 #pragma unroll
     for (int k = 0; k < BPT; k++) {
         if (jj[k] < 0) continue;
@@ -180,9 +189,12 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     const int rk = (int)cl.block_rank();
     const long img = blockIdx.x / C;
 
-    constexpr int twx = 0, twy = LX, A = LX + LY, B = LX + LY + G::FS;   // offsets in csm
-    for (int i = threadIdx.x; i < LX; i += kCT) csm[twx + i] = a.twx[i];
-    for (int i = threadIdx.x; i < LY; i += kCT) csm[twy + i] = a.twy[i];
+    // offsets in csm: stage twiddle tables of the x and y passes, fields A, B
+    constexpr int twx = 0, twy = G::TWX, A = G::TWX + G::TWY, B = A + G::FS;
+    for (int i = threadIdx.x; i < G::TWX; i += kCT)   // W_LX^{jm r}, r = i / X0 + 1, jm = i % X0
+        csm[twx + i] = a.twx[((i % X0) * (i / X0 + 1)) % LX];
+    for (int i = threadIdx.x; i < G::TWY; i += kCT)
+        csm[twy + i] = a.twy[((i % Y0) * (i / Y0 + 1)) % LY];
 
     const long M = G::M;
     const double Md = (double)M;
@@ -329,7 +341,7 @@ auto kernel_of() {
 template <int LX, int LY, int C>
 size_t cl_smem() {
     using G = CGeo<LX, LY, C, kCT>;
-    return sizeof(double2) * ((size_t)LX + LY + 2 * (size_t)G::FS);
+    return sizeof(double2) * ((size_t)G::TWX + G::TWY + 2 * (size_t)G::FS);
 }
 
 template <int LX, int LY, int C>
