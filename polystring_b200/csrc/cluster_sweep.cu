@@ -107,8 +107,11 @@ struct NoEpi {
 
 // One in-place pass over NL lines of this CTA's buffer: ad(l, n) is the index
 // of element n of line l; epi(l, n, value) gives what is stored at output n
-// (the pass's fused epilogue).  Starts and ends with the CTA synchronised.
-template <int N, int R, int NS, int SIGN, int NL, bool LFAST, class Ad, class Epi>
+// (the pass's fused epilogue).  The CTA synchronises after the loads and,
+// with TAIL, after the stores; without TAIL the caller orders the stores
+// before the next reads of this buffer (another pass's load barrier or a
+// cluster barrier).
+template <int N, int R, int NS, int SIGN, int NL, bool LFAST, bool TAIL, class Ad, class Epi>
 __device__ __noinline__ void local_pass(int buf, int tw, Ad ad, Epi epi) {
     constexpr int NB = N / R, TOTAL = NL * NB, BPT = (TOTAL + kCT - 1) / kCT;
     double2 v[BPT][R];
@@ -135,7 +138,7 @@ __device__ __noinline__ void local_pass(int buf, int tw, Ad ad, Epi epi) {
             csm[buf + ad(ll[k], n)] = epi(ll[k], n, v[k][r]);
         }
     }
-    __syncthreads();
+    if (TAIL) __syncthreads();
 }
 
 // The first radix pass of the other axis fused with the cluster transpose:
@@ -236,21 +239,41 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
                    (n % G::YC);
         };
     };
-    // forward y transform in row layout
-    auto fwd_y = [&](int fld) {
-        local_pass<LY, Y0, 1, -1, G::XR, true>(fld, twy, rowAd, NoEpi());
-        local_pass<LY, Y1, Y0, -1, G::XR, false>(fld, twy, rowAd, NoEpi());
+    // Forward y transform in row layout, of A and B with their passes
+    // interleaved (each pass's barrier after its loads also orders the other
+    // field's stores before the next pass on that field), or of B alone.  The
+    // transposes that follow start with a cluster barrier.
+    auto fwd_y2 = [&]() {
+        local_pass<LY, Y0, 1, -1, G::XR, true, false>(A, twy, rowAd, NoEpi());
+        local_pass<LY, Y0, 1, -1, G::XR, true, false>(B, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(A, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
     };
-    // x transform, k-space multiply by Lk, inverse x transform, in column layout
-    // (the first forward pass was the gather)
-    auto x_prop = [&](int fld, const double* Lk) {
-        auto kmul = [Lk, rk](int l, int n, double2 v) {
+    auto fwd_y1 = [&]() {
+        local_pass<LY, Y0, 1, -1, G::XR, true, true>(B, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
+    };
+    // x transform, k-space multiply by exp(-k^2 h) (fused into the last forward
+    // pass), inverse x transform, in column layout (the first forward pass was
+    // the gather): A with L1 and B with L2 interleaved, or B alone
+    auto kmul = [rk](const double* Lk) {
+        return [Lk, rk](int l, int n, double2 v) {
             const double f = __ldg(Lk + (long)n * LY + rk * G::YC + l);
             return make_double2(v.x * f, v.y * f);
         };
-        local_pass<LX, X1, X0, -1, G::YC, true>(fld, twx, colAd, kmul);
-        local_pass<LX, X0, 1, +1, G::YC, true>(fld, twx, colAd, NoEpi());
-        local_pass<LX, X1, X0, +1, G::YC, true>(fld, twx, colAd, NoEpi());
+    };
+    auto x_prop2 = [&]() {
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(A, twx, colAd, kmul(L1));
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(B, twx, colAd, kmul(L2));
+        local_pass<LX, X0, 1, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
+        local_pass<LX, X0, 1, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+        local_pass<LX, X1, X0, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
+        local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+    };
+    auto x_prop1 = [&]() {
+        local_pass<LX, X1, X0, -1, G::YC, true, true>(B, twx, colAd, kmul(L2));
+        local_pass<LX, X0, 1, +1, G::YC, true, true>(B, twx, colAd, NoEpi());
+        local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
     };
     // peers' rows -> first x pass -> this CTA's columns (both fields or one)
     auto rows_to_cols = [&](bool both) {
@@ -284,20 +307,18 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     for (int t = 0; t < a.Ns; t++) {
         const double *ef = eF(0, t), *ec = eF(1, t), *hfp = eH(0, t), *hcp = eH(1, t);
         // ---- full step (A, L1) and first half step (B, L2) ---------------------
-        fwd_y(A);
-        fwd_y(B);
+        fwd_y2();
         rows_to_cols(true);
-        x_prop(A, L1);
-        x_prop(B, L2);
+        x_prop2();
         cols_to_rows(true);
         // last inverse y pass; u = e^{-w ds/2} A / M stays in A,
         // B <- e^{-w ds/4} (e^{-w ds/4} B / M)
-        local_pass<LY, Y1, Y0, +1, G::XR, false>(A, twy, rowAd, [=](int l, int n, double2 v) {
+        local_pass<LY, Y1, Y0, +1, G::XR, false, false>(A, twy, rowAd, [=](int l, int n, double2 v) {
             const long g = g0 + l * LY + n;
             return make_double2(div_pow2_or_rn(v.x * __ldg(ef + g), Md, rMd, mpow2),
                                 div_pow2_or_rn(v.y * __ldg(ec + g), Md, rMd, mpow2));
         });
-        local_pass<LY, Y1, Y0, +1, G::XR, false>(B, twy, rowAd, [=](int l, int n, double2 v) {
+        local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
             const long g = g0 + l * LY + n;
             const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
             const double qtf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
@@ -305,9 +326,9 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
             return make_double2(ha * qtf, hb * qtc);
         });
         // ---- second half step (B, L2) -------------------------------------------
-        fwd_y(B);
+        fwd_y1();
         rows_to_cols(false);
-        x_prop(B, L2);
+        x_prop1();
         cols_to_rows(false);
         // last inverse y pass fused with q[t+1] = (4 qt2 - u) / 3, the history
         // write and the next step's inputs A = e^{-w ds/2} q, B = e^{-w ds/4} q
@@ -315,7 +336,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         const double *nf1 = eF(0, t + 1), *nc1 = eF(1, t + 1), *nf2 = eH(0, t + 1), *nc2 = eH(1, t + 1);
         double* of = hf + (long)(t + 1) * M;
         double* oc = hc + (long)(t + 1) * M;
-        local_pass<LY, Y1, Y0, +1, G::XR, false>(B, twy, rowAd, [=](int l, int n, double2 v) {
+        local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
             const long g = g0 + l * LY + n;
             const int si = rowAd(l, n);
             const double2 u = csm[A + si];
