@@ -94,3 +94,26 @@ def test_cluster_sweep_matches_line_passes(ps, shape, L, monkeypatch):
     np.testing.assert_allclose(Hc, Hl, rtol=1e-12, atol=0)
     assert np.abs(wc - wl).max() < 1e-11 * np.abs(wl).max()
     assert np.abs(pc - pl).max() < 1e-11
+
+
+def test_cluster_sweep_more_images_than_fit(ps, monkeypatch):
+    """64 images of 128^2 need 512 CTAs, more than are resident at once (48
+    clusters of 8): the clusters beyond run in later waves, with the same
+    results as the batched line passes; the tuning log reports the fit."""
+    from polystring_b200 import workloads
+    m, shape, L = 64, (128, 128, 1), 8.0
+    Ms = workloads.ms_from(0.35, 128)
+    wa, wb = workloads.string_images(m=m, shape=shape, L=L, seed=9)
+    out = {}
+    for path in ("cluster", "line_passes"):
+        if path == "line_passes":
+            monkeypatch.setenv("PS_B200_LINE_PASSES", "1")
+        g = ps.StringAB(m, 2, shape, ps.make_cell(2, "SQUARE", L), Ms, 18.0, max_iter=2)
+        g.set_images(wa, wb)
+        g.iterate(1)
+        out[path] = (g.H(), g.get("phiA"))
+        del g
+    log = ps.lib().ps_tuning_log().decode()
+    assert "cluster sweep: 8 CTAs per problem" in log and "batch 64" in log
+    np.testing.assert_allclose(out["cluster"][0], out["line_passes"][0], rtol=1e-12, atol=0)
+    assert np.abs(out["cluster"][1] - out["line_passes"][1]).max() < 1e-11
