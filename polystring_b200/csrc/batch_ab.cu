@@ -9,13 +9,19 @@
 // contour step t covers every solve that still has a step t (solves sorted by
 // Ns, so the active ones are a prefix), each CTA running the pass body of its
 // own solve (grouped_pass.cu).  Members are grouped by the number of grid
-// axes longer than one (2 or 3), which fixes the pass sequence of a step.  One
-// batch iteration -- all propagators, then every member's Q, densities and
-// field update -- is captured once as a CUDA graph and replayed.
+// axes longer than one (2 or 3), which fixes the pass sequence of a step.
+// Solves on grids with a persistent sweep take it instead: 32^3 and 48^3
+// solves of one shape share one cooperative launch for all their contour
+// steps (sweep.cu, a descriptor per solve, the CTAs split between solves),
+// 64^3 solves run their own 64^3 sweep (sweep64.cu), which fills the GPU
+// alone.  One batch iteration -- all propagators, then every member's Q,
+// densities and field update -- is captured once as a CUDA graph and
+// replayed.
 #include "batch_ab.h"
 
 #include <algorithm>
 #include <array>
+#include <map>
 #include <numeric>
 
 namespace ps {
@@ -46,6 +52,14 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             m_.push_back(new ModelAB(p, true));
             if (m_.back()->chain()->plan().naxes < 2) throw Error(-2, "batched solves need 2D or 3D grids");
         }
+        // persistent sweeps where the grid has one, grouped line passes for the rest
+        std::vector<int> swept, passes;
+        for (int k = 0; k < (int)m_.size(); k++) {
+            if (m_[k]->persistent_sweep64()) own_.push_back(k);
+            else if (m_[k]->persistent_sweep()) swept.push_back(k);
+            else passes.push_back(k);
+        }
+        build_sweeps(swept);
         // groups: same number of long axes (the step's pass sequence) and the
         // same schedule on each axis role (one kernel per grouped pass)
         auto key = [&](int k) {
@@ -54,13 +68,13 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
                                       pl.ax[pl.naxes - 1].reg};
         };
         std::vector<std::array<int, 4>> keys;
-        for (int k = 0; k < (int)m_.size(); k++)
+        for (int k : passes)
             if (std::find(keys.begin(), keys.end(), key(k)) == keys.end()) keys.push_back(key(k));
         for (const auto& kk : keys) {
             Group g;
             g.naxes = kk[0];
             g.path[0] = kk[1]; g.path[1] = kk[2]; g.path[2] = kk[3];
-            for (int k = 0; k < (int)m_.size(); k++)
+            for (int k : passes)
                 if (key(k) == kk) g.members.push_back(k);
             std::stable_sort(g.members.begin(), g.members.end(),
                              [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
@@ -68,24 +82,63 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             groups_.push_back(std::move(g));
         }
     } catch (...) {
-        for (auto* m : m_) delete m;
-        for (auto& g : groups_) {
-            cudaFree(g.dev);
-            for (auto* p : g.prefix_dev) cudaFree(p);
-        }
-        cudaStreamDestroy(st_);
+        release();
         throw;
     }
 }
 
-BatchAB::~BatchAB() {
+void BatchAB::release() {
     if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
     for (auto& g : groups_) {
         cudaFree(g.dev);
         for (auto* p : g.prefix_dev) cudaFree(p);
     }
+    for (auto& c : chunks_) {
+        cudaFree(c.dev);
+        cudaFree(c.bar);
+    }
     for (auto* m : m_) delete m;
+    m_.clear();
     if (st_) cudaStreamDestroy(st_);
+    st_ = nullptr;
+}
+
+BatchAB::~BatchAB() { release(); }
+
+void BatchAB::build_sweeps(const std::vector<int>& members) {
+    // shape -> solves, in member order
+    std::map<std::array<int, 3>, std::vector<int>> by_shape;
+    for (int k : members) {
+        const ModelABParams& p = m_[k]->params();
+        by_shape[{p.Lx, p.Ly, p.Lz}].push_back(k);
+    }
+    for (auto& kv : by_shape) {
+        const int Lx = kv.first[0], Ly = kv.first[1], Lz = kv.first[2];
+        const int resident = sweep_desc_prepare(Lx, Ly, Lz);
+        const int tasks = sweep_tasks_per_phase(Lx, Ly, Lz);
+        const std::vector<int>& ks = kv.second;
+        // at most one resident CTA per solve in a launch; more solves than
+        // resident CTAs go to further launches
+        for (size_t i0 = 0; i0 < ks.size(); i0 += (size_t)resident) {
+            chunks_.emplace_back();
+            SweepChunk& c = chunks_.back();
+            c.Lx = Lx; c.Ly = Ly; c.Lz = Lz;
+            c.n = (int)std::min(ks.size() - i0, (size_t)resident);
+            c.per = std::max(1, std::min(tasks, resident / c.n));
+            PS_CUDA(cudaMalloc(&c.bar, 32 * sizeof(unsigned) * (size_t)c.n));
+            std::vector<SweepArgs> d(c.n);
+            for (int i = 0; i < c.n; i++) {
+                d[i] = m_[ks[i0 + i]]->sweep_descriptor();
+                d[i].bar = c.bar + 32 * (size_t)i;
+                d[i].twx = twiddle_table(Lx);
+                d[i].twy = twiddle_table(Ly);
+                d[i].twz = twiddle_table(Lz);
+            }
+            PS_CUDA(cudaMalloc(&c.dev, sizeof(SweepArgs) * d.size()));
+            PS_CUDA(cudaMemcpy(c.dev, d.data(), sizeof(SweepArgs) * d.size(), cudaMemcpyHostToDevice));
+        }
+    }
 }
 
 void BatchAB::build_group(Group& g) {
@@ -130,6 +183,15 @@ void BatchAB::build_group(Group& g) {
 
 void BatchAB::enqueue_iteration() {
     int launches = 0;
+    for (const SweepChunk& c : chunks_) {
+        PS_CUDA(cudaMemsetAsync(c.bar, 0, 32 * sizeof(unsigned) * (size_t)c.n, st_));
+        sweep_launch_desc(c.dev, c.Lx, c.Ly, c.Lz, c.per, c.n, st_);
+        launches++;
+    }
+    for (int k : own_) {
+        m_[k]->enqueue_propagate(st_);
+        launches++;
+    }
     int Ns_max = 0;
     for (auto& g : groups_) Ns_max = std::max(Ns_max, g.Ns_max);
     for (int t = 0; t < Ns_max; t++) {

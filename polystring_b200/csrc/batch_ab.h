@@ -35,10 +35,21 @@ private:
         std::vector<int> prefix[9];
         size_t smem[9] = {};
     };
+    // solves of one shape with a generic persistent sweep, in one cooperative
+    // launch: n descriptors on the device, per CTAs a solve, n x 32 barrier words
+    struct SweepChunk {
+        int Lx = 0, Ly = 0, Lz = 0, per = 0, n = 0;
+        SweepArgs* dev = nullptr;
+        unsigned* bar = nullptr;
+    };
     void build_group(Group& g);
+    void build_sweeps(const std::vector<int>& members);
+    void release();
     void enqueue_iteration();
     std::vector<ModelAB*> m_;
     std::vector<Group> groups_;
+    std::vector<SweepChunk> chunks_;
+    std::vector<int> own_;                   // solves propagated by their own 64^3 sweep
     cudaStream_t st_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     int launches_ = 0;

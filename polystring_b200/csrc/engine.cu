@@ -402,7 +402,7 @@ ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
     }
     const char* force = getenv("PS_B200_LINE_PASSES");
     const char* generic = getenv("PS_B200_GENERIC_SWEEP");
-    const bool allow = !(force && force[0] == '1') && !batch_member;
+    const bool allow = !(force && force[0] == '1');
     use_sweep64_ = allow && p.mde == 0 && sweep64_supported(p.Lx, p.Ly, p.Lz) && !(generic && generic[0] == '1');
     use_sweep_ = allow && p.mde == 0 && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
     if (use_sweep64_) {
@@ -516,7 +516,23 @@ void ModelAB::set_fields(const double* wA, const double* wB, bool dev) {
     forward_done_ = false;
 }
 
-void ModelAB::enqueue_propagate() {
+SweepArgs ModelAB::sweep_descriptor() const {
+    if (!use_sweep_) throw Error(-2, "this solve has no generic persistent sweep");
+    SweepArgs a{};
+    a.hf = hf_.p; a.hc = hc_.p;
+    a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
+    a.uf = swU_.p; a.uc = swU_.p + M_;
+    a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
+    a.L1 = swL1_.p; a.L2 = swL2_.p;
+    a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
+    a.bar = swbar_; a.err = swerr_;
+    a.bstride_batch = 0; a.bstride_hist = 0; a.bstride_L = 0;
+    return a;
+}
+
+void ModelAB::enqueue_propagate() { enqueue_propagate(st_); }
+
+void ModelAB::enqueue_propagate(cudaStream_t s) {
     // propagators: forward chain qA -> qB, complementary chain qBc -> qAc
     // (Model_AB.cc:139-145, 187-193)
     if (use_sweep64_) {
@@ -527,27 +543,19 @@ void ModelAB::enqueue_propagate() {
         a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
         a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
         a.bar = swbar_; a.err = swerr_;
-        PS_CUDA(cudaMemsetAsync(swbar_, 0, 64 * sizeof(unsigned), st_));
-        sweep64_launch(a, swTab_.p, sweep_grid_, st_);
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 64 * sizeof(unsigned), s));
+        sweep64_launch(a, swTab_.p, sweep_grid_, s);
         return;
     }
     if (use_sweep_) {
-        SweepArgs a{};
-        a.hf = hf_.p; a.hc = hc_.p;
-        a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
-        a.uf = swU_.p; a.uc = swU_.p + M_;
-        a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
-        a.L1 = swL1_.p; a.L2 = swL2_.p;
-        a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
-        a.bar = swbar_; a.err = swerr_;
-        a.bstride_batch = 0; a.bstride_hist = 0; a.bstride_L = 0;
-        PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), st_));
-        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, st_);
+        const SweepArgs a = sweep_descriptor();
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), s));
+        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, s);
         return;
     }
     LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
     LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
-    chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, st_);
+    chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, s);
 }
 
 void ModelAB::enqueue_post(cudaStream_t st) {

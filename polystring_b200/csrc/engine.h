@@ -139,8 +139,9 @@ struct ModelABParams {
 
 class ModelAB {
 public:
-    // batch_member: the propagators run in grouped launches of a BatchAB
-    // (line passes, no persistent sweep, no tile tuning of its own)
+    // batch_member: the propagators run in launches of a BatchAB (persistent
+    // sweeps where the shape has one, else grouped line passes; no tile
+    // tuning of its own)
     explicit ModelAB(const ModelABParams& p, bool batch_member = false);
     ~ModelAB();
     void set_fields(const double* wA, const double* wB, bool device_ptrs);
@@ -164,7 +165,14 @@ public:
     int Ns() const { return Ns_; }
     long iterations() const { return iter_; }
     int status();
-    bool persistent_sweep() const { return use_sweep_; }
+    const ModelABParams& params() const { return p_; }
+    bool persistent_sweep() const { return use_sweep_; }       // generic sweep (sweep.cu)
+    bool persistent_sweep64() const { return use_sweep64_; }   // 64^3 sweep (sweep64.cu)
+    // the generic sweep's arguments for this solve (its own pointers, batch
+    // strides 0, its barrier words and error flag)
+    SweepArgs sweep_descriptor() const;
+    // the propagator sweeps of one iteration on stream s
+    void enqueue_propagate(cudaStream_t s);
     // Adjoint of the forward map (wA, wB) -> (phiA, phiB, Q) at fixed fields:
     // forward_only() evaluates the map; grad_w() returns the gradient (per
     // point of M) of sum(phiA_bar phiA + phiB_bar phiB) + Q_bar Q with respect

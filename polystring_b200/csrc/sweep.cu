@@ -111,8 +111,10 @@ __device__ __forceinline__ void plane_fft(double2* buf, const double2* twy, cons
     }
 }
 
+// The sweep of one problem; bidx scales the batch strides of a (the problem's
+// index in a strided batch, 0 when a describes the problem by its own pointers).
 template <int LX, int LY, int LZ>
-__global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
+__device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
     using G = Geo<LX, LY, LZ>;
     extern __shared__ double2 sm[];
     double2* twx = sm;
@@ -130,20 +132,20 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
     const double rMd = 1.0 / Md;
     const bool mpow2 = (M & (M - 1)) == 0;   // x / M == x * (1 / M) exactly
     const int nb = gridDim.x;
-    const long boff = (long)blockIdx.y * a.bstride_batch;   // batch offset of per-problem arrays
+    const long boff = bidx * a.bstride_batch;   // batch offset of per-problem arrays
     unsigned bar_target = 0;
-    unsigned* bar = a.bar + 32 * blockIdx.y;
+    unsigned* bar = a.bar + 32 * bidx;
     const int Ns = a.Ns;
 
-    double* hf = a.hf + (long)blockIdx.y * a.bstride_hist;
-    double* hc = a.hc + (long)blockIdx.y * a.bstride_hist;
+    double* hf = a.hf + bidx * a.bstride_hist;
+    double* hc = a.hc + bidx * a.bstride_hist;
     double2* Z1 = a.Z1 + boff;
     double2* Z2 = a.Z2 + boff;
     double2* Z3 = a.Z3 + boff;
     double* uf = a.uf + boff;
     double* uc = a.uc + boff;
-    const double* L1 = a.L1 + (long)blockIdx.y * a.bstride_L;
-    const double* L2 = a.L2 + (long)blockIdx.y * a.bstride_L;
+    const double* L1 = a.L1 + bidx * a.bstride_L;
+    const double* L2 = a.L2 + bidx * a.bstride_L;
     auto eF = [&](int lane, int t) -> const double* {   // e^{-w ds/2} of the lane's block at step t
         int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
         return (blk == 0 ? a.eFA : a.eFB) + boff;
@@ -339,6 +341,19 @@ __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
     }
 }
 
+// a strided batch: problem blockIdx.y at blockIdx.y times the strides of a
+template <int LX, int LY, int LZ>
+__global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
+    sweep_body<LX, LY, LZ>(a, blockIdx.y);
+}
+
+// a batch of independent problems, problem blockIdx.y described by d[blockIdx.y]
+template <int LX, int LY, int LZ>
+__global__ void __launch_bounds__(kNT, 1) sweep_rqm4_desc_kernel(const SweepArgs* __restrict__ d) {
+    const SweepArgs a = d[blockIdx.y];
+    sweep_body<LX, LY, LZ>(a, 0);
+}
+
 template <int LX, int LY, int LZ>
 size_t smem_bytes() {
     using G = Geo<LX, LY, LZ>;
@@ -350,12 +365,16 @@ int sweep_prepare_t(int* grid_out) {
     const size_t smem = smem_bytes<LX, LY, LZ>();
     PS_CUDA(cudaFuncSetAttribute(sweep_rqm4_kernel<LX, LY, LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-    int dev = 0, sms = 0, occ = 0;
+    PS_CUDA(cudaFuncSetAttribute(sweep_rqm4_desc_kernel<LX, LY, LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    int dev = 0, sms = 0, occ = 0, occ_d = 0;
     PS_CUDA(cudaGetDevice(&dev));
     PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_rqm4_kernel<LX, LY, LZ>, kNT, smem));
-    if (occ < 1) throw Error(-2, "sweep kernel does not fit on an SM");
-    *grid_out = sms * occ;
+    PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, sweep_rqm4_desc_kernel<LX, LY, LZ>, kNT, smem));
+    if (occ < 1 || occ_d < 1) throw Error(-2, "sweep kernel does not fit on an SM");
+    grid_out[0] = sms * occ;
+    grid_out[1] = sms * occ_d;
     twiddle_table(LX); twiddle_table(LY); twiddle_table(LZ);
     return 0;
 }
@@ -378,6 +397,21 @@ void sweep_launch_t(SweepArgs a, int grid, int nbatch, cudaStream_t st) {
     PS_CUDA(cudaLaunchKernelEx(&cfg, sweep_rqm4_kernel<LX, LY, LZ>, a));
 }
 
+template <int LX, int LY, int LZ>
+void sweep_launch_desc_t(const SweepArgs* d, int per, int n, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)per, (unsigned)n, 1);
+    cfg.blockDim = dim3(kNT, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes<LX, LY, LZ>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PS_CUDA(cudaLaunchKernelEx(&cfg, sweep_rqm4_desc_kernel<LX, LY, LZ>, d));
+}
+
 }  // namespace
 
 #define PS_SWEEP_SHAPES(X) \
@@ -391,8 +425,8 @@ bool sweep_supported(int Lx, int Ly, int Lz) {
 }
 
 int sweep_prepare(int Lx, int Ly, int Lz) {
-    int grid = 0;
-#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { sweep_prepare_t<a, b, c>(&grid); return grid; }
+    int grid[2] = {0, 0};
+#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { sweep_prepare_t<a, b, c>(grid); return grid[0]; }
     PS_SWEEP_SHAPES(PS_X)
 #undef PS_X
     throw Error(-2, "no persistent sweep for this grid");
@@ -400,6 +434,29 @@ int sweep_prepare(int Lx, int Ly, int Lz) {
 
 void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st) {
 #define PS_X(x, y, z) if (Lx == x && Ly == y && Lz == z) { sweep_launch_t<x, y, z>(a, grid, nbatch, st); return; }
+    PS_SWEEP_SHAPES(PS_X)
+#undef PS_X
+    throw Error(-2, "no persistent sweep for this grid");
+}
+
+int sweep_desc_prepare(int Lx, int Ly, int Lz) {
+    int grid[2] = {0, 0};
+#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { sweep_prepare_t<a, b, c>(grid); return grid[1]; }
+    PS_SWEEP_SHAPES(PS_X)
+#undef PS_X
+    throw Error(-2, "no persistent sweep for this grid");
+}
+
+int sweep_tasks_per_phase(int Lx, int Ly, int Lz) {
+#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { using G = Geo<a, b, c>; \
+        return 2 * G::NPT > G::NXT ? 2 * G::NPT : G::NXT; }
+    PS_SWEEP_SHAPES(PS_X)
+#undef PS_X
+    throw Error(-2, "no persistent sweep for this grid");
+}
+
+void sweep_launch_desc(const SweepArgs* d, int Lx, int Ly, int Lz, int per, int n, cudaStream_t st) {
+#define PS_X(x, y, z) if (Lx == x && Ly == y && Lz == z) { sweep_launch_desc_t<x, y, z>(d, per, n, st); return; }
     PS_SWEEP_SHAPES(PS_X)
 #undef PS_X
     throw Error(-2, "no persistent sweep for this grid");

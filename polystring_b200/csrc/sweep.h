@@ -29,6 +29,15 @@ void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStre
 // sets kernel attributes, builds twiddles; returns the cooperative grid size
 int sweep_prepare(int Lx, int Ly, int Lz);
 void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st);
+// Independent problems of one shape in one cooperative launch: d (device
+// memory) holds n descriptors with their own pointers (batch strides 0, bar =
+// 32 zeroed words each), per CTAs work on each problem (per * n must not
+// exceed sweep_desc_prepare's count of resident CTAs).  Problem k runs
+// d[k].Ns steps; the twiddle pointers come from twiddle_table.
+int sweep_desc_prepare(int Lx, int Ly, int Lz);
+// plane tasks / x tiles of the busiest phase: CTAs one problem can keep busy
+int sweep_tasks_per_phase(int Lx, int Ly, int Lz);
+void sweep_launch_desc(const SweepArgs* d, int Lx, int Ly, int Lz, int per, int n, cudaStream_t st);
 // batches of 2D problems, one thread-block cluster per problem (cluster_sweep.cu):
 // uses hf, hc, the factors, L1, L2, LA, LB, Ns and the batch strides of SweepArgs
 bool cluster_sweep_supported(int Lx, int Ly, int Lz);

@@ -98,3 +98,45 @@ def test_batch_rejects_what_it_cannot_run(ps):
     with pytest.raises(ps.PSError) as e:
         b.update(1)
     assert e.value.code == -6
+
+
+# cubic members take persistent sweeps: 32^3 and 48^3 solves of one shape share
+# one cooperative launch (uneven Ns), 64^3 runs its own 64^3 sweep; a 16^3
+# member stays on grouped line passes
+CUBIC = [
+    (3, (32, 32, 32), (3.8, 3.8, 3.8), (13, 21), 20.0, "Anderson"),
+    (3, (32, 32, 32), (4.1, 4.1, 4.1), (31, 43), 16.0, "EM"),
+    (3, (48, 48, 48), (4.4, 4.4, 4.4), (7, 13), 24.0, "EM"),
+    (3, (64, 64, 64), (4.2, 4.2, 4.2), (9, 17), 18.0, "Anderson"),
+    (3, (48, 48, 48), (3.9, 3.9, 3.9), (21, 33), 18.0, "Anderson"),
+    (3, (16, 16, 16), (3.6, 3.6, 3.6), (11, 15), 20.0, "EM"),
+]
+
+
+def _cubic(ps, s):
+    dim, shape, L, Ms, chiN, scft = s
+    return dict(dim=dim, shape=shape, cell=ps.make_cell(3, "CUBIC", L[0]), Ms=Ms, chiN=chiN, scft=scft,
+                n_anderson=4)
+
+
+def test_batch_sweep_members_follow_their_single_solves_exactly(ps, monkeypatch):
+    monkeypatch.setenv("PS_B200_AUTOTUNE", "0")
+    b = ps.BatchAB([_cubic(ps, s) for s in CUBIC])
+    singles = []
+    for k, s in enumerate(CUBIC):
+        wA, wB = _fields(s[1], 200 + k)
+        b.set_fields(k, wA, wB)
+        m = ps.ModelAB(**_cubic(ps, s))
+        m.set_fields(wA, wB)
+        singles.append(m)
+    for n in (1, 2):
+        b.update(n)
+        # 2 shared sweep launches (32^3, 48^3), one 64^3 sweep, grouped passes
+        # for the 16^3 member (Ns 24): fewer launches than the longest member
+        # (Ns 72) would need alone on per-step passes
+        assert 0 < b.launches_per_iteration() < 8 * 72
+        for k, m in enumerate(singles):
+            m.update(n)
+            assert b.H(k) == m.H(), (k, b.H(k), m.H())
+            for f in ("phiA", "phiB", "wA", "wB"):
+                assert np.array_equal(b.get(k, f), m.get(f)), (k, f)
