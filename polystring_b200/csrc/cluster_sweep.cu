@@ -67,6 +67,9 @@ struct CGeo {
     static constexpr long M = (long)LX * LY;
     static constexpr int TWX = (Plan2<LX>::r1 - 1) * Plan2<LX>::r0;   // stage twiddles (x passes)
     static constexpr int TWY = (Plan2<LY>::r1 - 1) * Plan2<LY>::r0;
+    // per-axis k factors (doubles): x full, y full, x half, y half, after the fields
+    static constexpr int KT = TWX + TWY + 2 * FS;          // offset in double2
+    static constexpr int NKT = 2 * (LX + LY);              // doubles
     static_assert(LX % C == 0 && LY % C == 0, "C must divide both axes");
     static_assert(E % NT == 0 && E / NT >= 1, "whole points per thread");
     static_assert(LX * YC == E && E <= FS, "column layout fits the row buffer");
@@ -198,6 +201,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         csm[twx + i] = a.twx[((i % X0) * (i / X0 + 1)) % LX];
     for (int i = threadIdx.x; i < G::TWY; i += kCT)
         csm[twy + i] = a.twy[((i % Y0) * (i / Y0 + 1)) % LY];
+    for (int i = threadIdx.x; i < G::NKT; i += kCT) reinterpret_cast<double*>(csm + G::KT)[i] = a.ktab[i];
 
     const long M = G::M;
     const double Md = (double)M;
@@ -206,8 +210,6 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     const long boff = img * a.bstride_batch;
     double* hf = a.hf + img * a.bstride_hist;
     double* hc = a.hc + img * a.bstride_hist;
-    const double* L1 = a.L1 + img * a.bstride_L;
-    const double* L2 = a.L2 + img * a.bstride_L;
     const long g0 = (long)rk * G::E;         // this CTA's rows in natural order
     auto eF = [&](int lane, int t) -> const double* {   // e^{-w ds/2} of the lane's block at step t
         int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
@@ -256,22 +258,25 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     // x transform, k-space multiply by exp(-k^2 h) (fused into the last forward
     // pass), inverse x transform, in column layout (the first forward pass was
     // the gather): A with L1 and B with L2 interleaved, or B alone
-    auto kmul = [rk](const double* Lk) {
-        return [Lk, rk](int l, int n, double2 v) {
-            const double f = __ldg(Lk + (long)n * LY + rk * G::YC + l);
+    // (orthogonal cells: exp(h (k_x^2 + k_y^2)) as the product of per-axis
+    // factors kept in shared memory, half = 0 for the full step, 1 for ds/2)
+    auto kmul = [rk](int half) {
+        return [rk, half](int l, int n, double2 v) {
+            const double* kt = reinterpret_cast<const double*>(csm + G::KT) + half * (LX + LY);
+            const double f = kt[n] * kt[LX + rk * G::YC + l];
             return make_double2(v.x * f, v.y * f);
         };
     };
     auto x_prop2 = [&]() {
-        local_pass<LX, X1, X0, -1, G::YC, true, false>(A, twx, colAd, kmul(L1));
-        local_pass<LX, X1, X0, -1, G::YC, true, false>(B, twx, colAd, kmul(L2));
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(A, twx, colAd, kmul(0));
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(B, twx, colAd, kmul(1));
         local_pass<LX, X0, 1, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
         local_pass<LX, X0, 1, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
         local_pass<LX, X1, X0, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
         local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
     };
     auto x_prop1 = [&]() {
-        local_pass<LX, X1, X0, -1, G::YC, true, true>(B, twx, colAd, kmul(L2));
+        local_pass<LX, X1, X0, -1, G::YC, true, true>(B, twx, colAd, kmul(1));
         local_pass<LX, X0, 1, +1, G::YC, true, true>(B, twx, colAd, NoEpi());
         local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
     };
@@ -336,20 +341,42 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         const double *nf1 = eF(0, t + 1), *nc1 = eF(1, t + 1), *nf2 = eH(0, t + 1), *nc2 = eH(1, t + 1);
         double* of = hf + (long)(t + 1) * M;
         double* oc = hc + (long)(t + 1) * M;
-        local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
+        // (three straight-line variants, chosen once per step: the last step
+        // prepares no next inputs, and the next step's e^{-w ds/4} tables are
+        // this step's unless a chain crosses its block boundary at t + 1)
+        auto fin = [=](int l, int n, double2 v, const double* gf2, const double* gc2, bool reuse) {
             const long g = g0 + l * LY + n;
             const int si = rowAd(l, n);
             const double2 u = csm[A + si];
-            double qf = div_pow2_or_rn(v.x * __ldg(hfp + g), Md, rMd, mpow2);
-            double qc = div_pow2_or_rn(v.y * __ldg(hcp + g), Md, rMd, mpow2);
+            const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
+            double qf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
+            double qc = div_pow2_or_rn(v.y * hb, Md, rMd, mpow2);
             qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
             qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
             of[g] = qf;
             oc[g] = qc;
-            if (!next) return v;
             csm[A + si] = make_double2(__ldg(nf1 + g) * qf, __ldg(nc1 + g) * qc);
-            return make_double2(__ldg(nf2 + g) * qf, __ldg(nc2 + g) * qc);
-        });
+            if (reuse) return make_double2(ha * qf, hb * qc);
+            return make_double2(__ldg(gf2 + g) * qf, __ldg(gc2 + g) * qc);
+        };
+        if (!next) {
+            local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
+                const long g = g0 + l * LY + n;
+                const int si = rowAd(l, n);
+                const double2 u = csm[A + si];
+                double qf = div_pow2_or_rn(v.x * __ldg(hfp + g), Md, rMd, mpow2);
+                double qc = div_pow2_or_rn(v.y * __ldg(hcp + g), Md, rMd, mpow2);
+                of[g] = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
+                oc[g] = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
+                return v;
+            });
+        } else if (nf2 == hfp && nc2 == hcp) {
+            local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd,
+                [=](int l, int n, double2 v) { return fin(l, n, v, nullptr, nullptr, true); });
+        } else {
+            local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd,
+                [=](int l, int n, double2 v) { return fin(l, n, v, nf2, nc2, false); });
+        }
     }
     cl.sync();   // no peer reads this CTA's shared memory after it exits
 }
@@ -362,7 +389,7 @@ auto kernel_of() {
 template <int LX, int LY, int C>
 size_t cl_smem() {
     using G = CGeo<LX, LY, C, kCT>;
-    return sizeof(double2) * ((size_t)G::TWX + G::TWY + 2 * (size_t)G::FS);
+    return sizeof(double2) * (size_t)G::KT + sizeof(double) * (size_t)G::NKT;
 }
 
 template <int LX, int LY, int C>

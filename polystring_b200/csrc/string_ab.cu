@@ -204,10 +204,15 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
         if (cluster_sweep_supported(p.Lx, p.Ly, p.Lz) && !(force && force[0] == '1')) {
             use_cluster_ = true;
             cluster_sweep_prepare(p.Lx, p.Ly, p.Lz, m);
-            clL1_.alloc(M_);
-            clL2_.alloc(M_);
-            PS_CUDA(cudaMemcpy(clL1_.p, L1.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
-            PS_CUDA(cudaMemcpy(clL2_.p, L2.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+            // per-axis factors exp(h k_x^2), exp(h k_y^2) for h = ds, ds/2: the
+            // orthogonal k2 along each axis (the other indices 0)
+            std::vector<double> kt;
+            for (double h : {dsA_, 0.5 * dsA_}) {
+                for (int x = 0; x < p.Lx; x++) kt.push_back(exp(h * k2[(long)x * p.Ly * p.Lz]));
+                for (int y = 0; y < p.Ly; y++) kt.push_back(exp(h * k2[(long)y * p.Lz]));
+            }
+            clK_.alloc(kt.size());
+            PS_CUDA(cudaMemcpy(clK_.p, kt.data(), sizeof(double) * kt.size(), cudaMemcpyHostToDevice));
         }
     }
     if (!use_cluster_) chain_->autotune(st_);
@@ -259,7 +264,7 @@ void StringAB::enqueue_scft_iteration() {
         SweepArgs a{};
         a.hf = hf_.p; a.hc = hc_.p;
         a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
-        a.L1 = clL1_.p; a.L2 = clL2_.p;
+        a.ktab = clK_.p;
         a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
         a.bstride_batch = M_; a.bstride_hist = hstride; a.bstride_L = 0;
         cluster_sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, m_, st_);

@@ -39,7 +39,7 @@ private:
     DevBuf hf_, hc_, wa_, wb_, yita_, phiA_, phiB_, eFA_, eHA_, eFB_, eHB_, ends_, cA_, cB_, scal_, S_, partial_;
     // one thread-block cluster per image for the propagators (2D grids that have one)
     bool use_cluster_ = false;
-    DevBuf clL1_, clL2_;                 // exp(ds k2), exp(ds k2 / 2) in natural order
+    DevBuf clK_;                         // per-axis exp(h k^2): x, y for h = ds, then ds / 2
     long iters_ = 0;
     bool ready_ = false;
 };

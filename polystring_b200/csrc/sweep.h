@@ -18,6 +18,7 @@ struct SweepArgs {
     long bstride_batch;              // per-problem stride of M-sized arrays
     long bstride_hist;               // per-problem stride of the histories
     long bstride_L;                  // per-problem stride of the k tables (0: shared)
+    const double* ktab;              // cluster sweep: per-axis exp(h k_x^2), exp(h k_y^2), h = ds then ds/2
 };
 
 bool sweep_supported(int Lx, int Ly, int Lz);
@@ -39,7 +40,8 @@ int sweep_desc_prepare(int Lx, int Ly, int Lz);
 int sweep_tasks_per_phase(int Lx, int Ly, int Lz);
 void sweep_launch_desc(const SweepArgs* d, int Lx, int Ly, int Lz, int per, int n, cudaStream_t st);
 // batches of 2D problems, one thread-block cluster per problem (cluster_sweep.cu):
-// uses hf, hc, the factors, L1, L2, LA, LB, Ns and the batch strides of SweepArgs
+// uses hf, hc, the factors, ktab (2 (Lx + Ly) doubles), LA, LB, Ns and the
+// batch strides of SweepArgs
 bool cluster_sweep_supported(int Lx, int Ly, int Lz);
 // sets kernel attributes, builds twiddles; returns how many clusters fit at once
 int cluster_sweep_prepare(int Lx, int Ly, int Lz, int nbatch);
