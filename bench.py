@@ -124,34 +124,75 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(cfg, seconds, threads):
-    """Time the CPU oracle (the restatement of the reference's step sequence)
-    on a bounded sample of the workload: RQM4 contour steps of one 64^3
-    propagator, as many as fit in `seconds` (about 95% of an SCFT iteration
-    is propagation)."""
+def cpu_propagation_rate(dim, shape, lengths, Ms, w, seconds, threads):
+    """Gridpoint contour steps per second of the CPU oracle's RQM4 propagator
+    (the restatement of the reference's step sequence) on one field of the
+    given grid: as many steps as fit in about `seconds`."""
     import oracle
     oracle.build()
     oracle.set_threads(threads)
-    shape = cfg["shape"]
     M = int(np.prod(shape))
-    L = cfg["cell"][1][0]
-    sA, sB = cfg["Ms"]
-    Ns = sA + sB - 2
-    k2 = oracle.k2_orthogonal(3, (L, L, L), shape)
-    ds = 1.0 / Ns
-    u = oracle.Updater("RQM4", k2, shape, ds)
-    qs = np.ones((2,) + shape)
+    Ns = Ms[0] + Ms[1] - 2
+    k2 = oracle.k2_orthogonal(dim, tuple(lengths), shape)
+    u = oracle.Updater("RQM4", k2, shape, 1.0 / Ns)
+    qs = np.ones((2,) + tuple(shape))
     t0 = time.perf_counter()
-    u.solve(cfg["wA"], qs)
+    u.solve(w, qs)
     one = time.perf_counter() - t0
     nsteps = max(1, int(seconds / max(one, 1e-6)))
-    qs = np.ones((nsteps + 1,) + shape)
+    qs = np.ones((nsteps + 1,) + tuple(shape))
     t0 = time.perf_counter()
-    u.solve(cfg["wA"], qs)
+    u.solve(w, qs)
     dt = time.perf_counter() - t0
-    return {"value": nsteps * M / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return nsteps * M / dt, nsteps, dt
+
+
+def cpu_baseline(cfg, seconds, threads):
+    """Time the CPU oracle on a bounded sample of the workload: RQM4 contour
+    steps of one 64^3 propagator, as many as fit in `seconds` (about 95% of an
+    SCFT iteration is propagation)."""
+    L = cfg["cell"][1][0]
+    rate, nsteps, dt = cpu_propagation_rate(3, cfg["shape"], (L, L, L), cfg["Ms"], cfg["wA"], seconds, threads)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": "%d RQM4 contour steps of one 64^3 propagator (oracle/scft_oracle.c, own FFT, "
                       "%d OpenMP threads), %.1f s" % (nsteps, threads, dt)}
+
+
+def cpu_string_baseline(seconds, threads, m=40, max_iter=3):
+    """The string section's CPU leg: the oracle's RQM4 steps on one 128^2
+    image, converted to string iterations per second of the 40-image C3
+    string (2 Ns steps per image per SCFT iteration).  Propagation only, about
+    95% of the work, so the CPU rate is if anything overstated."""
+    from polystring_b200 import workloads
+    shape, L = (128, 128, 1), 8.0
+    Ms = workloads.ms_from(0.35, 128)
+    wa, _ = workloads.string_images(m=m, shape=shape, L=L)
+    rate, nsteps, dt = cpu_propagation_rate(2, shape, (L, L), Ms, wa[m // 2], seconds, threads)
+    work = m * max_iter * 2 * (Ms[0] + Ms[1] - 2) * int(np.prod(shape))
+    return {"string_iters_per_s": rate / work, "gridpt_steps_per_s": rate, "cores": threads, "kind": "port",
+            "sample": "%d RQM4 steps of one 128^2 image propagator (oracle, %d OpenMP threads), %.1f s; "
+                      "propagation only" % (nsteps, threads, dt)}
+
+
+def cpu_batch_baseline(seconds, threads, n=27):
+    """The uneven batch's CPU leg: the oracle's RQM4 rate on each grid of the
+    sample (seconds split between them), applied to every solve's 2 Ns M
+    steps, as one host process running the solves one after another would."""
+    from polystring_b200 import workloads
+    specs = workloads.uneven_solves(n)
+    rates, samples = {}, []
+    shapes = sorted({tuple(sp["shape"]) for sp in specs})
+    for shp in shapes:
+        sp = next(x for x in specs if tuple(x["shape"]) == shp)
+        L = sp["cell"][1][0]
+        r, nsteps, dt = cpu_propagation_rate(3, shp, (L, L, L), sp["Ms"], sp["wA"], seconds / len(shapes), threads)
+        rates[shp] = r
+        samples.append("%d steps at %d^3 in %.1f s" % (nsteps, shp[0], dt))
+    work = [2 * (sp["Ms"][0] + sp["Ms"][1] - 2) * int(np.prod(sp["shape"])) for sp in specs]
+    t = sum(w / rates[tuple(sp["shape"])] for w, sp in zip(work, specs))
+    return {"gridpt_steps_per_s": sum(work) / t, "cores": threads, "kind": "port",
+            "sample": "oracle RQM4 propagators, %d OpenMP threads: %s; propagation only"
+                      % (threads, ", ".join(samples))}
 
 
 def string_method(ps, iters=10):
@@ -493,6 +534,10 @@ def main():
     if rank == 0 and world == 1:
         import oracle
         cpu = cpu_baseline(cfg, args.cpu_seconds, oracle.max_threads())
+        if string is not None:
+            string["cpu_baseline"] = cpu_string_baseline(0.5 * args.cpu_seconds, oracle.max_threads())
+        if batch is not None:
+            batch["cpu_baseline"] = cpu_batch_baseline(0.5 * args.cpu_seconds, oracle.max_threads())
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
