@@ -140,3 +140,24 @@ def test_batch_sweep_members_follow_their_single_solves_exactly(ps, monkeypatch)
             assert b.H(k) == m.H(), (k, b.H(k), m.H())
             for f in ("phiA", "phiB", "wA", "wB"):
                 assert np.array_equal(b.get(k, f), m.get(f)), (k, f)
+
+
+def test_batch_sweep_chunks_beyond_resident_ctas(ps, monkeypatch):
+    """149 solves of 32^3 need more CTAs than the generic sweep keeps resident
+    (one per SM): they split into several cooperative launches (one CTA a
+    solve in a full one) and still follow their single solves exactly."""
+    monkeypatch.setenv("PS_B200_AUTOTUNE", "0")
+    n = 149
+    spec = lambda k: dict(dim=3, shape=(32, 32, 32), cell=ps.make_cell(3, "CUBIC", 3.8 + 0.01 * (k % 7)),
+                          Ms=(5, 7 + (k % 3)), chiN=18.0 + 0.1 * (k % 5), scft="EM")
+    b = ps.BatchAB([spec(k) for k in range(n)])
+    fields = [_fields((32, 32, 32), 300 + k) for k in range(n)]
+    for k in range(n):
+        b.set_fields(k, *fields[k])
+    b.update(2)
+    for k in (0, 147, 148):
+        m = ps.ModelAB(**spec(k))
+        m.set_fields(*fields[k])
+        m.update(2)
+        assert b.H(k) == m.H(), (k, b.H(k), m.H())
+        assert np.array_equal(b.get(k, "phiA"), m.get("phiA")), k
