@@ -117,14 +117,19 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
         const int Lx = kv.first[0], Ly = kv.first[1], Lz = kv.first[2];
         const int resident = sweep_desc_prepare(Lx, Ly, Lz);
         const int tasks = sweep_tasks_per_phase(Lx, Ly, Lz);
-        const std::vector<int>& ks = kv.second;
-        // at most one resident CTA per solve in a launch; more solves than
-        // resident CTAs go to further launches
-        for (size_t i0 = 0; i0 < ks.size(); i0 += (size_t)resident) {
+        // A launch lasts as long as its longest solve, and a solve given fewer
+        // CTAs than it has tasks per phase takes several rounds a phase: so a
+        // launch holds only as many solves as can each have all the CTAs they
+        // can use (9 at 32^3, 1 at 48^3 with 148 resident CTAs), taken in
+        // order of Ns so that solves of similar length share a launch.
+        std::vector<int> ks = kv.second;
+        std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
+        const size_t cap = (size_t)std::max(1, resident / tasks);
+        for (size_t i0 = 0; i0 < ks.size(); i0 += cap) {
             chunks_.emplace_back();
             SweepChunk& c = chunks_.back();
             c.Lx = Lx; c.Ly = Ly; c.Lz = Lz;
-            c.n = (int)std::min(ks.size() - i0, (size_t)resident);
+            c.n = (int)std::min(ks.size() - i0, cap);
             c.per = std::max(1, std::min(tasks, resident / c.n));
             PS_CUDA(cudaMalloc(&c.bar, 32 * sizeof(unsigned) * (size_t)c.n));
             std::vector<SweepArgs> d(c.n);

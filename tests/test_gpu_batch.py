@@ -143,9 +143,9 @@ def test_batch_sweep_members_follow_their_single_solves_exactly(ps, monkeypatch)
 
 
 def test_batch_sweep_chunks_beyond_resident_ctas(ps, monkeypatch):
-    """149 solves of 32^3 need more CTAs than the generic sweep keeps resident
-    (one per SM): they split into several cooperative launches (one CTA a
-    solve in a full one) and still follow their single solves exactly."""
+    """149 solves of 32^3 split into several cooperative launches (as many
+    solves a launch as can each have the 16 CTAs a 32^3 sweep keeps busy,
+    taken in order of Ns) and still follow their single solves exactly."""
     monkeypatch.setenv("PS_B200_AUTOTUNE", "0")
     n = 149
     spec = lambda k: dict(dim=3, shape=(32, 32, 32), cell=ps.make_cell(3, "CUBIC", 3.8 + 0.01 * (k % 7)),
