@@ -117,20 +117,34 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
         const int Lx = kv.first[0], Ly = kv.first[1], Lz = kv.first[2];
         const int resident = sweep_desc_prepare(Lx, Ly, Lz);
         const int tasks = sweep_tasks_per_phase(Lx, Ly, Lz);
-        // A launch lasts as long as its longest solve, and a solve given fewer
-        // CTAs than it has tasks per phase takes several rounds a phase: so a
-        // launch holds only as many solves as can each have all the CTAs they
-        // can use (9 at 32^3, 1 at 48^3 with 148 resident CTAs), taken in
-        // order of Ns so that solves of similar length share a launch.
+        // A launch of n solves gives each per = resident / n CTAs (at most the
+        // tasks of a phase) and lasts its longest solve's Ns steps, each step
+        // sweep_rounds_per_step(per) rounds of tasks.  With the solves in
+        // order of Ns, the launches are consecutive runs of that order; pick
+        // the runs with the least total cost (dynamic programme over n).
         std::vector<int> ks = kv.second;
         std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
-        const size_t cap = (size_t)std::max(1, resident / tasks);
-        for (size_t i0 = 0; i0 < ks.size(); i0 += cap) {
+        const int nk = (int)ks.size();
+        auto per_of = [&](int n) { return std::max(1, std::min(tasks, resident / n)); };
+        std::vector<double> best(nk + 1, 0.0);
+        std::vector<int> from(nk + 1, 0);
+        for (int i = 1; i <= nk; i++) {
+            best[i] = -1.0;
+            for (int j = std::max(0, i - resident); j < i; j++) {
+                const double c = best[j] + (double)m_[ks[j]]->Ns() * sweep_rounds_per_step(Lx, Ly, Lz, per_of(i - j));
+                if (best[i] < 0.0 || c < best[i]) { best[i] = c; from[i] = j; }
+            }
+        }
+        std::vector<std::pair<int, int>> runs;   // [i0, i1) in ks
+        for (int i = nk; i > 0; i = from[i]) runs.push_back({from[i], i});
+        std::reverse(runs.begin(), runs.end());
+        for (const auto& run : runs) {
+            const size_t i0 = (size_t)run.first;
             chunks_.emplace_back();
             SweepChunk& c = chunks_.back();
             c.Lx = Lx; c.Ly = Ly; c.Lz = Lz;
-            c.n = (int)std::min(ks.size() - i0, cap);
-            c.per = std::max(1, std::min(tasks, resident / c.n));
+            c.n = run.second - run.first;
+            c.per = per_of(c.n);
             PS_CUDA(cudaMalloc(&c.bar, 32 * sizeof(unsigned) * (size_t)c.n));
             std::vector<SweepArgs> d(c.n);
             for (int i = 0; i < c.n; i++) {

@@ -455,6 +455,15 @@ int sweep_tasks_per_phase(int Lx, int Ly, int Lz) {
     throw Error(-2, "no persistent sweep for this grid");
 }
 
+int sweep_rounds_per_step(int Lx, int Ly, int Lz, int per) {
+    if (per < 1) per = 1;
+#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { using G = Geo<a, b, c>; \
+        return 2 * ((G::NXT + per - 1) / per) + 2 * ((2 * G::NPT + per - 1) / per); }
+    PS_SWEEP_SHAPES(PS_X)
+#undef PS_X
+    throw Error(-2, "no persistent sweep for this grid");
+}
+
 void sweep_launch_desc(const SweepArgs* d, int Lx, int Ly, int Lz, int per, int n, cudaStream_t st) {
 #define PS_X(x, y, z) if (Lx == x && Ly == y && Lz == z) { sweep_launch_desc_t<x, y, z>(d, per, n, st); return; }
     PS_SWEEP_SHAPES(PS_X)

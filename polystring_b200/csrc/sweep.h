@@ -38,6 +38,9 @@ void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbat
 int sweep_desc_prepare(int Lx, int Ly, int Lz);
 // plane tasks / x tiles of the busiest phase: CTAs one problem can keep busy
 int sweep_tasks_per_phase(int Lx, int Ly, int Lz);
+// rounds of tasks per contour step (two x-passes, two plane phases) when one
+// problem has per CTAs: the step time in units of a task
+int sweep_rounds_per_step(int Lx, int Ly, int Lz, int per);
 void sweep_launch_desc(const SweepArgs* d, int Lx, int Ly, int Lz, int per, int n, cudaStream_t st);
 // batches of 2D problems, one thread-block cluster per problem (cluster_sweep.cu):
 // uses hf, hc, the factors, ktab (2 (Lx + Ly) doubles), LA, LB, Ns and the
