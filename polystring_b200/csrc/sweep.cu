@@ -66,9 +66,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, int* err, unsigned
     return stop == 0;
 }
 
-// in-place line FFTs with register staging (smem_line_fft.cuh), kNT threads
+// in-place line FFTs with register staging (smem_line_fft.cuh), kNT threads;
+// 48-point lines in two passes (16 then 3) rather than the three of Plan<48>
+// (measured: 48^3 contour step 79 -> 65 us)
+struct Plan16x3 { static constexpr int P = 2, r0 = 16, r1 = 3, r2 = 1; };
+template <int N> struct SweepPlan { using type = Plan<N>; };
+template <> struct SweepPlan<48> { using type = Plan16x3; };
 template <int N, int NL, int ES, class Off, int SIGN>
-using LineFFT = SmemLineFFT<N, NL, ES, Off, SIGN, kNT>;
+using LineFFT = SmemLineFFT<N, NL, ES, Off, SIGN, kNT, typename SweepPlan<N>::type>;
 
 constexpr int largest_div_le(int n, int cap) {
     int t = cap < n ? cap : n;
