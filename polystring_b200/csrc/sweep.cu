@@ -30,7 +30,8 @@ namespace ps {
 
 namespace {
 
-constexpr int kNT = 512;                 // threads per CTA
+constexpr int kNT = 512;                 // threads per CTA (one problem a launch)
+constexpr int kNTB = 256;                // threads per CTA of the descriptor batches (2 CTAs an SM)
 constexpr long long kSpinLimit = 20000000; // polls before a barrier gives up
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -66,14 +67,14 @@ __device__ __forceinline__ bool grid_barrier(unsigned* count, int* err, unsigned
     return stop == 0;
 }
 
-// in-place line FFTs with register staging (smem_line_fft.cuh), kNT threads;
+// in-place line FFTs with register staging (smem_line_fft.cuh), NT threads;
 // 48-point lines in two passes (16 then 3) rather than the three of Plan<48>
 // (measured: 48^3 contour step 79 -> 65 us)
 struct Plan16x3 { static constexpr int P = 2, r0 = 16, r1 = 3, r2 = 1; };
 template <int N> struct SweepPlan { using type = Plan<N>; };
 template <> struct SweepPlan<48> { using type = Plan16x3; };
-template <int N, int NL, int ES, class Off, int SIGN>
-using LineFFT = SmemLineFFT<N, NL, ES, Off, SIGN, kNT, typename SweepPlan<N>::type>;
+template <int N, int NL, int ES, class Off, int SIGN, int NT>
+using LineFFT = SmemLineFFT<N, NL, ES, Off, SIGN, NT, typename SweepPlan<N>::type>;
 
 constexpr int largest_div_le(int n, int cap) {
     int t = cap < n ? cap : n;
@@ -91,7 +92,6 @@ struct Geo {
     static constexpr int ZP = (LZ > 1 && LZ % 2 == 0) ? LZ + 1 : LZ;  // smem row pitch
     static constexpr int XT = largest_div_le(P, (2048 + LX - 1) / LX);  // columns per x tile
     static constexpr int NXT = P / XT;                      // x tiles
-    static constexpr int EPT = (PT + kNT - 1) / kNT;        // plane elements per thread
     static constexpr int PLANE_SMEM = PR * LY * ZP;         // double2
     static constexpr int XTILE_SMEM = 2 * LX * XT;          // double2 (two fields)
     static constexpr int SMEM = (PLANE_SMEM > XTILE_SMEM ? PLANE_SMEM : XTILE_SMEM);
@@ -103,33 +103,36 @@ __device__ __forceinline__ int pidx(int p) {
     return (p / LZ) * G::ZP + (p % LZ);
 }
 
-template <int LX, int LY, int LZ, int SIGN>
+template <int LX, int LY, int LZ, int SIGN, int NT>
 __device__ __forceinline__ void plane_fft(double2* buf, const double2* twy, const double2* twz) {
     using G = Geo<LX, LY, LZ>;
     if constexpr (LZ > 1) {
         // z lines: line l = (pr, y), element z at l*ZP + z
-        LineFFT<LZ, G::PR * LY, 1, OffMul<G::ZP>, SIGN>::run(buf, twz, OffMul<G::ZP>());
+        LineFFT<LZ, G::PR * LY, 1, OffMul<G::ZP>, SIGN, NT>::run(buf, twz, OffMul<G::ZP>());
     }
     if constexpr (LY > 1) {
         // y lines: line l = (pr, z), element y at pr*LY*ZP + y*ZP + z
-        LineFFT<LY, G::PR * LZ, G::ZP, OffSplit<LZ, LY * G::ZP>, SIGN>::run(buf, twy, OffSplit<LZ, LY * G::ZP>());
+        LineFFT<LY, G::PR * LZ, G::ZP, OffSplit<LZ, LY * G::ZP>, SIGN, NT>::run(buf, twy, OffSplit<LZ, LY * G::ZP>());
     }
 }
 
 // The sweep of one problem; bidx scales the batch strides of a (the problem's
-// index in a strided batch, 0 when a describes the problem by its own pointers).
-template <int LX, int LY, int LZ>
+// index in a strided batch, 0 when a describes the problem by its own pointers);
+// NT threads a CTA (the thread count changes which thread computes what, not
+// the arithmetic).
+template <int LX, int LY, int LZ, int NT>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
     using G = Geo<LX, LY, LZ>;
+    constexpr int EPT = (G::PT + NT - 1) / NT;   // plane elements per thread
     extern __shared__ double2 sm[];
     double2* twx = sm;
     double2* twy = twx + LX;
     double2* twz = twy + LY;
     double2* buf = twz + LZ;
 
-    for (int m = threadIdx.x; m < LX; m += kNT) twx[m] = a.twx[m];
-    for (int m = threadIdx.x; m < LY; m += kNT) twy[m] = a.twy[m];
-    for (int m = threadIdx.x; m < LZ; m += kNT) twz[m] = a.twz[m];
+    for (int m = threadIdx.x; m < LX; m += NT) twx[m] = a.twx[m];
+    for (int m = threadIdx.x; m < LY; m += NT) twy[m] = a.twy[m];
+    for (int m = threadIdx.x; m < LZ; m += NT) twz[m] = a.twz[m];
     __syncthreads();
 
     const long M = G::M;
@@ -163,17 +166,17 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
     // ---- plane task helpers -------------------------------------------------
     auto load_plane = [&](const double2* Z, long slab0) {
 #pragma unroll 4
-        for (int k = 0; k < G::EPT; k++) {
-            int p = threadIdx.x + k * kNT;
-            if (G::PT % kNT == 0 || p < G::PT) buf[pidx<G, LZ>(p)] = Z[slab0 + p];
+        for (int k = 0; k < EPT; k++) {
+            int p = threadIdx.x + k * NT;
+            if (G::PT % NT == 0 || p < G::PT) buf[pidx<G, LZ>(p)] = Z[slab0 + p];
         }
         __syncthreads();
     };
     auto store_plane = [&](double2* Z, long slab0) {
 #pragma unroll 4
-        for (int k = 0; k < G::EPT; k++) {
-            int p = threadIdx.x + k * kNT;
-            if (G::PT % kNT == 0 || p < G::PT) Z[slab0 + p] = buf[pidx<G, LZ>(p)];
+        for (int k = 0; k < EPT; k++) {
+            int p = threadIdx.x + k * NT;
+            if (G::PT % NT == 0 || p < G::PT) Z[slab0 + p] = buf[pidx<G, LZ>(p)];
         }
     };
 
@@ -184,15 +187,15 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
         const double* ef = role == 0 ? eF(0, 0) : eH(0, 0);
         const double* ec = role == 0 ? eF(1, 0) : eH(1, 0);
 #pragma unroll 2
-        for (int k = 0; k < G::EPT; k++) {
-            int p = threadIdx.x + k * kNT;
-            if (G::PT % kNT == 0 || p < G::PT) {
+        for (int k = 0; k < EPT; k++) {
+            int p = threadIdx.x + k * NT;
+            if (G::PT % NT == 0 || p < G::PT) {
                 long g = s0 + p;
                 buf[pidx<G, LZ>(p)] = make_double2(ef[g] * hf[g], ec[g] * hc[g]);
             }
         }
         __syncthreads();
-        plane_fft<LX, LY, LZ, -1>(buf, twy, twz);
+        plane_fft<LX, LY, LZ, -1, NT>(buf, twy, twz);
         store_plane(role == 0 ? Z1 : Z2, s0);
         __syncthreads();
     }
@@ -207,14 +210,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                 const long c0 = (long)task * G::XT;
                 // load: element (x, c) of field f at buf[f*LX*XT + x*XT + c]
                 constexpr int XE = LX * G::XT;
-                constexpr int XEPT = (XE + kNT - 1) / kNT;
+                constexpr int XEPT = (XE + NT - 1) / NT;
                 for (int f = 0; f < nf; f++) {
                     const double2* Z = phase == 0 ? (f == 0 ? Z1 : Z2) : Z3;
                     double2* xb = buf + f * XE;
 #pragma unroll 2
                     for (int k = 0; k < XEPT; k++) {
-                        int e = threadIdx.x + k * kNT;
-                        if (XE % kNT == 0 || e < XE) {
+                        int e = threadIdx.x + k * NT;
+                        if (XE % NT == 0 || e < XE) {
                             int x = e / G::XT, c = e % G::XT;
                             xb[e] = Z[(long)x * G::P + c0 + c];
                         }
@@ -223,12 +226,12 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                 __syncthreads();
                 for (int f = 0; f < nf; f++) {
                     double2* xb = buf + f * XE;
-                    LineFFT<LX, G::XT, G::XT, OffMul<1>, -1>::run(xb, twx, OffMul<1>());
+                    LineFFT<LX, G::XT, G::XT, OffMul<1>, -1, NT>::run(xb, twx, OffMul<1>());
                     const double* L = (phase == 0 && f == 0) ? L1 : L2;
 #pragma unroll 2
                     for (int k = 0; k < XEPT; k++) {
-                        int e = threadIdx.x + k * kNT;
-                        if (XE % kNT == 0 || e < XE) {
+                        int e = threadIdx.x + k * NT;
+                        if (XE % NT == 0 || e < XE) {
                             int x = e / G::XT, c = e % G::XT;
                             double lv = L[(long)x * G::P + c0 + c];
                             double2 v = xb[e];
@@ -236,15 +239,15 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                         }
                     }
                     __syncthreads();
-                    LineFFT<LX, G::XT, G::XT, OffMul<1>, +1>::run(xb, twx, OffMul<1>());
+                    LineFFT<LX, G::XT, G::XT, OffMul<1>, +1, NT>::run(xb, twx, OffMul<1>());
                 }
                 for (int f = 0; f < nf; f++) {
                     double2* Z = phase == 0 ? (f == 0 ? Z1 : Z2) : Z3;
                     double2* xb = buf + f * XE;
 #pragma unroll 2
                     for (int k = 0; k < XEPT; k++) {
-                        int e = threadIdx.x + k * kNT;
-                        if (XE % kNT == 0 || e < XE) {
+                        int e = threadIdx.x + k * NT;
+                        if (XE % NT == 0 || e < XE) {
                             int x = e / G::XT, c = e % G::XT;
                             Z[(long)x * G::P + c0 + c] = xb[e];
                         }
@@ -261,14 +264,14 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                     const int role = task / G::NPT;
                     const long s0 = (long)(task % G::NPT) * G::PT;
                     load_plane(role == 0 ? Z1 : Z2, s0);
-                    plane_fft<LX, LY, LZ, +1>(buf, twy, twz);
+                    plane_fft<LX, LY, LZ, +1, NT>(buf, twy, twz);
                     if (role == 0) {
                         const double* ef = eF(0, t);
                         const double* ec = eF(1, t);
 #pragma unroll 2
-                        for (int k = 0; k < G::EPT; k++) {
-                            int p = threadIdx.x + k * kNT;
-                            if (G::PT % kNT == 0 || p < G::PT) {
+                        for (int k = 0; k < EPT; k++) {
+                            int p = threadIdx.x + k * NT;
+                            if (G::PT % NT == 0 || p < G::PT) {
                                 long g = s0 + p;
                                 double2 v = buf[pidx<G, LZ>(p)];
                                 uf[g] = div_pow2_or_rn(v.x * ef[g], Md, rMd, mpow2);
@@ -280,9 +283,9 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                         const double* hfp = eH(0, t);
                         const double* hcp = eH(1, t);
 #pragma unroll 2
-                        for (int k = 0; k < G::EPT; k++) {
-                            int p = threadIdx.x + k * kNT;
-                            if (G::PT % kNT == 0 || p < G::PT) {
+                        for (int k = 0; k < EPT; k++) {
+                            int p = threadIdx.x + k * NT;
+                            if (G::PT % NT == 0 || p < G::PT) {
                                 long g = s0 + p;
                                 int si = pidx<G, LZ>(p);
                                 double2 v = buf[si];
@@ -293,7 +296,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
                             }
                         }
                         __syncthreads();
-                        plane_fft<LX, LY, LZ, -1>(buf, twy, twz);
+                        plane_fft<LX, LY, LZ, -1, NT>(buf, twy, twz);
                         store_plane(Z3, s0);
                         __syncthreads();
                     }
@@ -310,7 +313,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
             const long s0 = (long)(task % G::NPT) * G::PT;
             if (!next && role == 1) continue;
             load_plane(Z3, s0);
-            plane_fft<LX, LY, LZ, +1>(buf, twy, twz);
+            plane_fft<LX, LY, LZ, +1, NT>(buf, twy, twz);
             const double* hfp = eH(0, t);
             const double* hcp = eH(1, t);
             const double* nf = next ? (role == 0 ? eF(0, t + 1) : eH(0, t + 1)) : nullptr;
@@ -318,9 +321,9 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
             double* of = hf + (long)(t + 1) * M;
             double* oc = hc + (long)(t + 1) * M;
 #pragma unroll 2
-            for (int k = 0; k < G::EPT; k++) {
-                int p = threadIdx.x + k * kNT;
-                if (G::PT % kNT == 0 || p < G::PT) {
+            for (int k = 0; k < EPT; k++) {
+                int p = threadIdx.x + k * NT;
+                if (G::PT % NT == 0 || p < G::PT) {
                     long g = s0 + p;
                     int si = pidx<G, LZ>(p);
                     double2 v = buf[si];
@@ -334,7 +337,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
             }
             __syncthreads();
             if (next) {
-                plane_fft<LX, LY, LZ, -1>(buf, twy, twz);
+                plane_fft<LX, LY, LZ, -1, NT>(buf, twy, twz);
                 store_plane(role == 0 ? Z1 : Z2, s0);
                 __syncthreads();
             }
@@ -349,14 +352,16 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
 // a strided batch: problem blockIdx.y at blockIdx.y times the strides of a
 template <int LX, int LY, int LZ>
 __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
-    sweep_body<LX, LY, LZ>(a, blockIdx.y);
+    sweep_body<LX, LY, LZ, kNT>(a, blockIdx.y);
 }
 
 // a batch of independent problems, problem blockIdx.y described by d[blockIdx.y]
 template <int LX, int LY, int LZ>
-__global__ void __launch_bounds__(kNT, 1) sweep_rqm4_desc_kernel(const SweepArgs* __restrict__ d) {
+// (kNTB threads, two CTAs an SM: more solves share the GPU at full width;
+// measured on the C5 sample 8.65e9 -> 9.71e9 gridpt*steps/s)
+__global__ void __launch_bounds__(kNTB, 2) sweep_rqm4_desc_kernel(const SweepArgs* __restrict__ d) {
     const SweepArgs a = d[blockIdx.y];
-    sweep_body<LX, LY, LZ>(a, 0);
+    sweep_body<LX, LY, LZ, kNTB>(a, 0);
 }
 
 template <int LX, int LY, int LZ>
@@ -376,7 +381,7 @@ int sweep_prepare_t(int* grid_out) {
     PS_CUDA(cudaGetDevice(&dev));
     PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_rqm4_kernel<LX, LY, LZ>, kNT, smem));
-    PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, sweep_rqm4_desc_kernel<LX, LY, LZ>, kNT, smem));
+    PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, sweep_rqm4_desc_kernel<LX, LY, LZ>, kNTB, smem));
     if (occ < 1 || occ_d < 1) throw Error(-2, "sweep kernel does not fit on an SM");
     grid_out[0] = sms * occ;
     grid_out[1] = sms * occ_d;
@@ -406,7 +411,7 @@ template <int LX, int LY, int LZ>
 void sweep_launch_desc_t(const SweepArgs* d, int per, int n, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)per, (unsigned)n, 1);
-    cfg.blockDim = dim3(kNT, 1, 1);
+    cfg.blockDim = dim3(kNTB, 1, 1);
     cfg.dynamicSmemBytes = smem_bytes<LX, LY, LZ>();
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
