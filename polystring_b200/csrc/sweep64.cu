@@ -42,9 +42,13 @@ constexpr long long kSpin = 20000000;
 // shared memory map (bytes)
 constexpr int OFF_PLANE = 0;                                   // 64 x 65 double2 (also x-pass scratch)
 constexpr int SZ_PLANE = 64 * PITCH * 16;
-constexpr int OFF_EHA = OFF_PLANE + SZ_PLANE;                  // 4096 double
-constexpr int OFF_EHB = OFF_EHA + P64 * 8;
-constexpr int OFF_U = OFF_EHB + P64 * 8;                       // 4096 double2
+// the slab's e^{-w ds/4} tables, row pitch EHP doubles: a warp reads 4 rows x 8
+// consecutive z, and a pitch of 72 (not 64) puts alternate rows on the other
+// 16 banks (2 wavefronts a read instead of 4)
+constexpr int EHP = 72;
+constexpr int OFF_EHA = OFF_PLANE + SZ_PLANE;                  // 64 x EHP double
+constexpr int OFF_EHB = OFF_EHA + 64 * EHP * 8;
+constexpr int OFF_U = OFF_EHB + 64 * EHP * 8;                  // 4096 double2 (16-byte aligned)
 constexpr int OFF_TW = OFF_U + P64 * 16;                       // 64 double2
 constexpr int OFF_TAB = OFF_TW + 64 * 16;                      // 6 x 64 double: x,y,z tables for L1 then L2
 constexpr int OFF_MBAR = OFF_TAB + 6 * 64 * 8;                 // mbarrier (8 B)
@@ -254,8 +258,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     for (int i = tid; i < 6 * 64; i += NT) tab[i] = tables[i];
     if (planar) {
         for (int i = tid; i < P64; i += NT) {
-            ehA[i] = a.eHA[soff + i];
-            ehB[i] = a.eHB[soff + i];
+            ehA[(i >> 6) * EHP + (i & 63)] = a.eHA[soff + i];
+            ehB[(i >> 6) * EHP + (i & 63)] = a.eHB[soff + i];
         }
     }
     if (tid == 0) mbar_init(mbar);
@@ -273,6 +277,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     auto eh_f = [&](int st) { return st < a.LA ? s.ehA : s.ehB; };
     auto eh_c = [&](int st) { return st < a.LB ? s.ehB : s.ehA; };
     const int zb = r * 64 + t;   // slab index of (y = r, z = t) ; + 8 k of z
+    const int zbe = r * EHP + t; // the same point in the factor tables
 
     // ---- step 0 forward transforms ----------------------------------------
     if (planar) {
@@ -281,8 +286,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
         double2 v[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            const int zi = zb + 8 * k;
-            double hf = ef[zi], hc = ec[zi];
+            const int zi = zb + 8 * k, ze = zbe + 8 * k;
+            double hf = ef[ze], hc = ec[ze];
             if (role == 0) { hf *= hf; hc *= hc; }
             v[k] = make_double2(hf * a.hf[soff + zi], hc * a.hc[soff + zi]);
         }
@@ -307,15 +312,15 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
             if (role == 0) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int zi = zb + 8 * k;
-                    double hf = ef[zi], hc = ec[zi];
+                    const int zi = zb + 8 * k, ze = zbe + 8 * k;
+                    double hf = ef[ze], hc = ec[ze];
                     ug[soff + zi] = make_double2((v[k].x * (hf * hf)) * rMd, (v[k].y * (hc * hc)) * rMd);
                 }
             } else {
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int zi = zb + 8 * k;
-                    double hf = ef[zi], hc = ec[zi];
+                    const int ze = zbe + 8 * k;
+                    double hf = ef[ze], hc = ec[ze];
                     double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
                     v[k] = make_double2(hf * qf, hc * qc);
                 }
@@ -349,15 +354,15 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
             double* oc = a.hc + (long)(st + 1) * M64 + soff;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int zi = zb + 8 * k;
-                double hf = ef[zi], hc = ec[zi];
+                const int zi = zb + 8 * k, ze = zbe + 8 * k;
+                double hf = ef[ze], hc = ec[ze];
                 double2 u = s.u[zi];
                 double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
                 qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
                 qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
                 if (role == 0) of[zi] = qf;
                 if (role == 1 || !next) oc[zi] = qc;
-                double gf = nf[zi], gc = nc[zi];
+                double gf = nf[ze], gc = nc[ze];
                 if (role == 0) { gf *= gf; gc *= gc; }
                 v[k] = make_double2(gf * qf, gc * qc);
             }
