@@ -16,7 +16,12 @@ static void pass(std::vector<double2>& in, std::vector<double2>& out, int L, con
     in.swap(out);
 }
 
-template <int N, int SIGN>
+// two-pass plans of particular kernels besides Plan<N> (48 in the generic
+// sweep, 128 in the string cluster sweep)
+struct Plan16x3 { static constexpr int P = 2, r0 = 16, r1 = 3, r2 = 1; };
+struct Plan16x8 { static constexpr int P = 2, r0 = 16, r1 = 8, r2 = 1; };
+
+template <int N, int SIGN, class PL = Plan<N>>
 static double run() {
     const int L = 3;
     std::vector<double2> a(N * L), b(N * L), ref(N * L);
@@ -41,10 +46,10 @@ static double run() {
             }
             ref[k * L + l] = mk((double)sr, (double)si);
         }
-    constexpr int r0 = Plan<N>::r0, r1 = Plan<N>::r1, r2 = Plan<N>::r2;
-    if (Plan<N>::P >= 1) pass<N, r0, 1, SIGN>(a, b, L, tw.data());
-    if (Plan<N>::P >= 2) pass<N, r1, r0, SIGN>(a, b, L, tw.data());
-    if (Plan<N>::P >= 3) pass<N, r2, r0 * r1, SIGN>(a, b, L, tw.data());
+    constexpr int r0 = PL::r0, r1 = PL::r1, r2 = PL::r2;
+    if (PL::P >= 1) pass<N, r0, 1, SIGN>(a, b, L, tw.data());
+    if (PL::P >= 2) pass<N, r1, r0, SIGN>(a, b, L, tw.data());
+    if (PL::P >= 3) pass<N, r2, r0 * r1, SIGN>(a, b, L, tw.data());
     double err = 0, mx = 0;
     for (int i = 0; i < N * L; i++) {
         err = fmax(err, fmax(fabs(a[i].x - ref[i].x), fabs(a[i].y - ref[i].y)));
@@ -121,5 +126,7 @@ int main() {
     e = fmax(e, run<256, -1>());
     e = fmax(e, run<8, 1>());    e = fmax(e, run<48, 1>());   e = fmax(e, run<64, 1>());
     e = fmax(e, run<128, 1>());  e = fmax(e, run<12, 1>());   e = fmax(e, run<256, 1>());
+    e = fmax(e, run<48, -1, Plan16x3>());  e = fmax(e, run<48, 1, Plan16x3>());
+    e = fmax(e, run<128, -1, Plan16x8>()); e = fmax(e, run<128, 1, Plan16x8>());
     return e < 1e-14 ? 0 : 1;
 }
