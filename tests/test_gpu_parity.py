@@ -1,7 +1,7 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
 
-Tolerances (FP64 throughout; north_star bar 1e-10 relative on Q and H and
-max-abs on the densities):
+Tolerances (FP64 throughout; the parity bar is 1e-10 relative on Q and H
+and max-abs on the densities):
 * single propagator solves: 1e-12 relative to max |q|;
 * one SCFT iteration and short trajectories: 1e-10;
 * converged free energies against the reference's published values: the
