@@ -222,8 +222,18 @@ def string_method(ps, iters=10):
         single.update(3)
         single.H()
     ts = time.perf_counter() - t0
+    # the whole string iteration as propagator work: 2 Ns steps of M points
+    # per image and SCFT iteration, 15 log2(M) + 20 FP64 flops each
+    import math
+    M = int(np.prod(shape))
+    rate = m * 3 * 2 * (Ms[0] + Ms[1] - 2) * M / tb
+    flop = 15.0 * math.log2(M) + 20.0
     return {"config": "C3 string, 40 images 128x128, Ms %s, 3 SCFT iterations per image" % list(Ms),
             "batched_string_iters_per_s": 1.0 / tb, "sequential_plain_gpu_iters_per_s": 1.0 / ts,
+            "gridpt_steps_per_s": rate,
+            "fp64": {"flop_per_gridpt_step": flop, "achieved_tflops": rate * flop / 1e12, "peak_tflops": 37.0,
+                     "peak_kind": "nominal", "frac": rate * flop / 37.0e12,
+                     "note": "whole string iteration (densities, mixing, spline included) counted as propagation"},
             "speedup_vs_sequential": ts / tb, "launches_per_string_iteration": g.launches_per_iteration(),
             "propagator_path": [l for l in ps.lib().ps_tuning_log().decode().split("\ngrid ") if "128x128x1" in l],
             "timing": "host wall clock around synchronised replays"}
