@@ -82,7 +82,8 @@ constexpr int largest_div_le(int n, int cap) {
     return t < 1 ? 1 : t;
 }
 
-template <int LX, int LY, int LZ>
+// XTC: elements per x line of an x tile at most (tile columns = XTC / LX)
+template <int LX, int LY, int LZ, int XTC = 2048>
 struct Geo {
     static constexpr int P = LY * LZ;                       // points per x-slab
     static constexpr long M = (long)LX * P;
@@ -90,7 +91,7 @@ struct Geo {
     static constexpr int PT = PR * P;                       // points per plane task
     static constexpr int NPT = LX / PR;                     // plane tasks per role
     static constexpr int ZP = (LZ > 1 && LZ % 2 == 0) ? LZ + 1 : LZ;  // smem row pitch
-    static constexpr int XT = largest_div_le(P, (2048 + LX - 1) / LX);  // columns per x tile
+    static constexpr int XT = largest_div_le(P, (XTC + LX - 1) / LX);  // columns per x tile
     static constexpr int NXT = P / XT;                      // x tiles
     static constexpr int PLANE_SMEM = PR * LY * ZP;         // double2
     static constexpr int XTILE_SMEM = 2 * LX * XT;          // double2 (two fields)
@@ -120,9 +121,16 @@ __device__ __forceinline__ void plane_fft(double2* buf, const double2* twy, cons
 // index in a strided batch, 0 when a describes the problem by its own pointers);
 // NT threads a CTA (the thread count changes which thread computes what, not
 // the arithmetic).
+// x tiles of a single 48^3 solve: 18 columns (128 tiles) rather than 36, so
+// more CTAs share its x passes (step 65 -> 57 us); the shared batch launches
+// keep 36 (they fill the GPU with several solves).  The tile never changes
+// the arithmetic, and shared memory is sized for the larger tile.
+template <int LX, int NT>
+constexpr int xtile_cap() { return (LX == 48 && NT == kNT) ? 1024 : 2048; }
+
 template <int LX, int LY, int LZ, int NT>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
-    using G = Geo<LX, LY, LZ>;
+    using G = Geo<LX, LY, LZ, xtile_cap<LX, NT>()>;
     constexpr int EPT = (G::PT + NT - 1) / NT;   // plane elements per thread
     extern __shared__ double2 sm[];
     double2* twx = sm;
