@@ -144,6 +144,57 @@ __device__ __noinline__ void local_pass(int buf, int tw, Ad ad, Epi epi) {
     if (TAIL) __syncthreads();
 }
 
+// The last pass of an inverse transform along the lines (radix R1 after
+// stages of R0, so butterfly jj holds the outputs jj + R0 r), a pointwise
+// epilogue, and the first pass of the next forward transform (radix R0, no
+// twiddles: butterfly j takes x[j + R1 r']), fused in registers: thread
+// (l, j), j < R1, runs the inverse butterflies j + R1 m (m < R0 / R1), whose
+// outputs are exactly forward butterfly j's inputs (r' = m + (R0 / R1) r).
+// epi(l, n, value) maps the inverse output at n to the forward input.  One
+// load barrier and one store barrier instead of two passes' four.
+template <int N, int R0, int R1, int NL, class Ad, class Epi>
+__device__ __noinline__ void inv_epi_fwd_pass(int buf, int tw, Ad ad, Epi epi) {
+    static_assert(R0 * R1 == N && R0 % R1 == 0, "two-pass plan with R1 dividing R0");
+    constexpr int Q = R0 / R1;
+    constexpr int TOTAL = NL * R1, BPT = (TOTAL + kCT - 1) / kCT;
+    double2 v[BPT][R0];
+    int ll[BPT], jj[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        const int b = threadIdx.x + k * kCT;
+        jj[k] = -1;
+        if (TOTAL % kCT == 0 || b < TOTAL) {
+            ll[k] = b / R1;
+            jj[k] = b % R1;
+#pragma unroll
+            for (int m = 0; m < Q; m++)
+#pragma unroll
+                for (int r = 0; r < R1; r++) v[k][m + Q * r] = csm[buf + ad(ll[k], jj[k] + R1 * m + R0 * r)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        if (jj[k] < 0) continue;
+        const int j = jj[k], l = ll[k];
+#pragma unroll
+        for (int m = 0; m < Q; m++) {
+            double2 w[R1];
+#pragma unroll
+            for (int r = 0; r < R1; r++) w[r] = v[k][m + Q * r];
+            butterfly<N, R1, R0, +1>(w, j + R1 * m, csm + tw);   // outputs at j + R1 m + R0 r
+#pragma unroll
+            for (int r = 0; r < R1; r++) v[k][m + Q * r] = w[r];
+        }
+#pragma unroll
+        for (int q = 0; q < R0; q++) v[k][q] = epi(l, j + R1 * q, v[k][q]);
+        butterfly<N, R0, 1, -1>(v[k], j, nullptr);                  // outputs at j R0 + r''
+#pragma unroll
+        for (int q = 0; q < R0; q++) csm[buf + ad(l, j * R0 + q)] = v[k][q];
+    }
+    __syncthreads();
+}
+
 // The first radix pass of the other axis fused with the cluster transpose:
 // the butterfly inputs come from the peers' buffers (src(l, n) points at
 // element n of line l there), the butterflies run in registers, a cluster
@@ -243,16 +294,12 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     };
     // Forward y transform in row layout, of A and B with their passes
     // interleaved (each pass's barrier after its loads also orders the other
-    // field's stores before the next pass on that field), or of B alone.  The
-    // transposes that follow start with a cluster barrier.
+    // field's stores before the next pass on that field).  The transposes that
+    // follow start with a cluster barrier.
     auto fwd_y2 = [&]() {
         local_pass<LY, Y0, 1, -1, G::XR, true, false>(A, twy, rowAd, NoEpi());
         local_pass<LY, Y0, 1, -1, G::XR, true, false>(B, twy, rowAd, NoEpi());
         local_pass<LY, Y1, Y0, -1, G::XR, false, false>(A, twy, rowAd, NoEpi());
-        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
-    };
-    auto fwd_y1 = [&]() {
-        local_pass<LY, Y0, 1, -1, G::XR, true, true>(B, twy, rowAd, NoEpi());
         local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
     };
     // x transform, k-space multiply by exp(-k^2 h) (fused into the last forward
@@ -323,7 +370,9 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
             return make_double2(div_pow2_or_rn(v.x * __ldg(ef + g), Md, rMd, mpow2),
                                 div_pow2_or_rn(v.y * __ldg(ec + g), Md, rMd, mpow2));
         });
-        local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
+        // (B's last inverse pass, its epilogue and the first forward pass of
+        // the second half step in one register-resident pass)
+        inv_epi_fwd_pass<LY, Y0, Y1, G::XR>(B, twy, rowAd, [=](int l, int n, double2 v) {
             const long g = g0 + l * LY + n;
             const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
             const double qtf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
@@ -331,7 +380,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
             return make_double2(ha * qtf, hb * qtc);
         });
         // ---- second half step (B, L2) -------------------------------------------
-        fwd_y1();
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
         rows_to_cols(false);
         x_prop1();
         cols_to_rows(false);
