@@ -195,6 +195,70 @@ __device__ __noinline__ void inv_epi_fwd_pass(int buf, int tw, Ad ad, Epi epi) {
     __syncthreads();
 }
 
+// The same fusion at the end of a contour step, with two outputs: epi(l, n,
+// value) returns the next step's inputs of both fields (.a for field A, .b
+// for field B) from B's inverse output at n, reading this CTA's field A at n
+// (the full-step result u).  B's forward outputs are stored after the load
+// barrier; A's only after a second barrier, once no thread reads u any more.
+struct FieldPair { double2 a, b; };
+template <int N, int R0, int R1, int NL, class Ad, class Epi>
+__device__ __noinline__ void inv_epi_fwd2_pass(int bufB, int bufA, int tw, Ad ad, Epi epi) {
+    static_assert(R0 * R1 == N && R0 % R1 == 0, "two-pass plan with R1 dividing R0");
+    constexpr int Q = R0 / R1;
+    constexpr int TOTAL = NL * R1, BPT = (TOTAL + kCT - 1) / kCT;
+    double2 v[BPT][R0];
+    int ll[BPT], jj[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        const int b = threadIdx.x + k * kCT;
+        jj[k] = -1;
+        if (TOTAL % kCT == 0 || b < TOTAL) {
+            ll[k] = b / R1;
+            jj[k] = b % R1;
+#pragma unroll
+            for (int m = 0; m < Q; m++)
+#pragma unroll
+                for (int r = 0; r < R1; r++) v[k][m + Q * r] = csm[bufB + ad(ll[k], jj[k] + R1 * m + R0 * r)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        if (jj[k] < 0) continue;
+        const int j = jj[k], l = ll[k];
+#pragma unroll
+        for (int m = 0; m < Q; m++) {
+            double2 w[R1];
+#pragma unroll
+            for (int r = 0; r < R1; r++) w[r] = v[k][m + Q * r];
+            butterfly<N, R1, R0, +1>(w, j + R1 * m, csm + tw);
+#pragma unroll
+            for (int r = 0; r < R1; r++) v[k][m + Q * r] = w[r];
+        }
+        double2 av[R0];
+#pragma unroll
+        for (int q = 0; q < R0; q++) {
+            const FieldPair pr = epi(l, j + R1 * q, v[k][q]);
+            av[q] = pr.a;
+            v[k][q] = pr.b;
+        }
+        butterfly<N, R0, 1, -1>(v[k], j, nullptr);
+#pragma unroll
+        for (int q = 0; q < R0; q++) csm[bufB + ad(l, j * R0 + q)] = v[k][q];
+        butterfly<N, R0, 1, -1>(av, j, nullptr);
+#pragma unroll
+        for (int q = 0; q < R0; q++) v[k][q] = av[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        if (jj[k] < 0) continue;
+#pragma unroll
+        for (int q = 0; q < R0; q++) csm[bufA + ad(ll[k], jj[k] * R0 + q)] = v[k][q];
+    }
+    __syncthreads();
+}
+
 // The first radix pass of the other axis fused with the cluster transpose:
 // the butterfly inputs come from the peers' buffers (src(l, n) points at
 // element n of line l there), the butterflies run in registers, a cluster
@@ -296,9 +360,12 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     // interleaved (each pass's barrier after its loads also orders the other
     // field's stores before the next pass on that field).  The transposes that
     // follow start with a cluster barrier.
-    auto fwd_y2 = [&]() {
-        local_pass<LY, Y0, 1, -1, G::XR, true, false>(A, twy, rowAd, NoEpi());
-        local_pass<LY, Y0, 1, -1, G::XR, true, false>(B, twy, rowAd, NoEpi());
+    // (after step 0 the first pass was fused into the previous step's end)
+    auto fwd_y2 = [&](bool first_pass) {
+        if (first_pass) {
+            local_pass<LY, Y0, 1, -1, G::XR, true, false>(A, twy, rowAd, NoEpi());
+            local_pass<LY, Y0, 1, -1, G::XR, true, false>(B, twy, rowAd, NoEpi());
+        }
         local_pass<LY, Y1, Y0, -1, G::XR, false, false>(A, twy, rowAd, NoEpi());
         local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
     };
@@ -359,7 +426,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     for (int t = 0; t < a.Ns; t++) {
         const double *ef = eF(0, t), *ec = eF(1, t), *hfp = eH(0, t), *hcp = eH(1, t);
         // ---- full step (A, L1) and first half step (B, L2) ---------------------
-        fwd_y2();
+        fwd_y2(t == 0);
         rows_to_cols(true);
         x_prop2();
         cols_to_rows(true);
@@ -395,8 +462,7 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
         // this step's unless a chain crosses its block boundary at t + 1)
         auto fin = [=](int l, int n, double2 v, const double* gf2, const double* gc2, bool reuse) {
             const long g = g0 + l * LY + n;
-            const int si = rowAd(l, n);
-            const double2 u = csm[A + si];
+            const double2 u = csm[A + rowAd(l, n)];
             const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
             double qf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
             double qc = div_pow2_or_rn(v.y * hb, Md, rMd, mpow2);
@@ -404,9 +470,10 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
             qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
             of[g] = qf;
             oc[g] = qc;
-            csm[A + si] = make_double2(__ldg(nf1 + g) * qf, __ldg(nc1 + g) * qc);
-            if (reuse) return make_double2(ha * qf, hb * qc);
-            return make_double2(__ldg(gf2 + g) * qf, __ldg(gc2 + g) * qc);
+            FieldPair p;
+            p.a = make_double2(__ldg(nf1 + g) * qf, __ldg(nc1 + g) * qc);
+            p.b = reuse ? make_double2(ha * qf, hb * qc) : make_double2(__ldg(gf2 + g) * qf, __ldg(gc2 + g) * qc);
+            return p;
         };
         if (!next) {
             local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd, [=](int l, int n, double2 v) {
@@ -420,10 +487,11 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
                 return v;
             });
         } else if (nf2 == hfp && nc2 == hcp) {
-            local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd,
+            // (with the next step's first forward pass of both fields)
+            inv_epi_fwd2_pass<LY, Y0, Y1, G::XR>(B, A, twy, rowAd,
                 [=](int l, int n, double2 v) { return fin(l, n, v, nullptr, nullptr, true); });
         } else {
-            local_pass<LY, Y1, Y0, +1, G::XR, false, true>(B, twy, rowAd,
+            inv_epi_fwd2_pass<LY, Y0, Y1, G::XR>(B, A, twy, rowAd,
                 [=](int l, int n, double2 v) { return fin(l, n, v, nf2, nc2, false); });
         }
     }
