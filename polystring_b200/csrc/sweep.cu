@@ -21,6 +21,13 @@
 // Grid barriers are counter based with a bounded spin: on timeout a CTA
 // raises the error flag, every CTA sees the flag and returns, and the host
 // reports the failure.  The launch is cooperative, so all CTAs are resident.
+//
+// Two launch forms share the body: one problem (or a strided batch) at 512
+// threads a CTA, one CTA an SM; and a batch of independent problems of one
+// shape described by per-problem descriptors (uneven batches), at 256
+// threads a CTA, two CTAs an SM.  The thread count and the x-tile width
+// change which thread computes what, never the arithmetic, so a batched
+// problem's results equal its single solve's bit for bit.
 #include "ps_internal.h"
 #include "fft_core.cuh"
 #include "smem_line_fft.cuh"
