@@ -1,0 +1,182 @@
+"""Oracle parity at the full sizes of the benchmark workloads.
+
+Every case compares the CUDA path (through the C ABI) with the CPU oracle on
+the same seeded inputs, at the parity bar: 1e-10 relative on Q and H,
+1e-10 max-abs on the densities and fields (FP64).
+
+* C1: 2D 64x64, Ms [31, 71], simple mixing lambda 0.1, the whole 500-iteration
+  trajectory, compared every 50 iterations (oracle run live).
+* C2: 3D 64^3, Ms [71, 131], Anderson (history 20): the first 5 iterations
+  live (histories too), and the long trajectory against the oracle's
+  committed fixture (tests/golden/make_trajectories.py).
+* C3: one string iteration of 40 images of 128x128, Ms [46, 84]
+  (Quad4_Closed on both blocks), three SCFT iterations per image.
+* C5: every member of the 27-solve uneven sample (32^3 / 48^3 / 64^3, Ns
+  64 / 128 / 256) for 2 Anderson iterations.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def ps():
+    oracle.build()
+    oracle.set_threads(oracle.max_threads())
+    import polystring_b200
+    return polystring_b200
+
+
+def _lengths(cfg):
+    system, a = cfg["cell"]
+    return tuple([a[0]] * cfg["dim"]) if system in ("SQUARE", "CUBIC") else tuple(a)
+
+
+def _pair(ps, cfg):
+    """(oracle model, GPU model) of a workload configuration, fields set."""
+    system, a = cfg["cell"]
+    cell = ps.make_cell(cfg["dim"], system, *a)
+    kw = dict(lam=cfg["lam"], mde=cfg["mde"], scft=cfg["scft"], n_anderson=cfg["n_anderson"])
+    o = oracle.ModelAB(cfg["dim"], cfg["shape"], _lengths(cfg), cfg["Ms"], cfg["chiN"], **kw)
+    m = ps.ModelAB(cfg["dim"], cfg["shape"], cell, cfg["Ms"], cfg["chiN"], **kw)
+    o.init_fields(cfg["wA"], cfg["wB"])
+    m.set_fields(cfg["wA"], cfg["wB"])
+    return o, m
+
+
+def _compare(o, m, tag, fields=("phiA", "phiB", "wA", "wB")):
+    assert abs(m.Q() - o.Q()) / o.Q() < 1e-10, (tag, m.Q(), o.Q())
+    Ho, Hg = o.H()[0], m.H()[0]
+    assert abs(Hg - Ho) / abs(Ho) < 1e-10, (tag, Hg, Ho)
+    for f in fields:
+        d = np.abs(m.get(f) - o.get(f)).max()
+        assert d < 1e-10, (tag, f, d)
+    assert abs(m.residual_error() - o.residual()) <= 1e-8 * o.residual(), (tag, m.residual_error(), o.residual())
+
+
+def test_c1_em_trajectory_matches_oracle(ps):
+    """C1: the whole 500-iteration simple-mixing trajectory."""
+    from polystring_b200 import workloads
+    cfg = workloads.config("C1")
+    o, m = _pair(ps, cfg)
+    for it in range(50, cfg["iters"] + 1, 50):
+        o.update(50)
+        m.update(50)
+        _compare(o, m, "C1 iteration %d" % it)
+
+
+def test_c2_first_iterations_match_oracle(ps):
+    """C2 at full size: Ns 200 on 64^3 with Anderson (history 20); H, Q,
+    densities and fields every iteration, the four histories after the first."""
+    from polystring_b200 import workloads
+    cfg = workloads.config("C2")
+    o, m = _pair(ps, cfg)
+    for it in range(1, 6):
+        o.update(1)
+        m.update(1)
+        _compare(o, m, "C2 iteration %d" % it)
+        if it == 1:
+            for f in ("qA", "qB", "qAc", "qBc"):
+                a, b = m.get(f), o.get(f)
+                assert np.abs(a - b).max() / np.abs(b).max() < 1e-12, f
+
+
+def _trajectory_fixture(name):
+    path = os.path.join(HERE, "golden", "%s_trajectory.npz" % name)
+    if not os.path.exists(path):
+        pytest.skip("no trajectory fixture %s" % path)
+    return np.load(path)
+
+
+def test_c2_long_trajectory_against_oracle_fixture(ps):
+    """C2's Anderson trajectory against the oracle's recorded one: H, Q after
+    every iteration, fields at sampled points every 100 iterations, for as
+    many iterations as the fixture holds (up to the workload's 1000)."""
+    from polystring_b200 import workloads
+    fx = _trajectory_fixture("c2")
+    cfg = workloads.config("C2")
+    system, a = cfg["cell"]
+    m = ps.ModelAB(3, cfg["shape"], ps.make_cell(3, system, *a), cfg["Ms"], cfg["chiN"], lam=cfg["lam"],
+                   mde=cfg["mde"], scft=cfg["scft"], n_anderson=cfg["n_anderson"])
+    m.set_fields(cfg["wA"], cfg["wB"])
+    scal = fx["scalars"]
+    every = int(fx["every"])
+    idx = fx["sample_index"]
+    worst, first_over = 0.0, None
+    for k in range(1, scal.shape[0] + 1):
+        m.update(1)
+        eH = abs(m.H()[0] - scal[k - 1, 0]) / abs(scal[k - 1, 0])
+        eQ = abs(m.Q() - scal[k - 1, 3]) / scal[k - 1, 3]
+        e = max(eH, eQ)
+        worst = max(worst, e)
+        if e > 1e-10 and first_over is None:
+            first_over = k
+        j = k // every - 1
+        if k % every == 0 and j < len(fx["wA_sample"]):
+            for f in ("wA", "wB", "phiA", "phiB"):
+                d = np.abs(m.get(f).ravel()[idx] - fx[f + "_sample"][j]).max()
+                assert d < 1e-10, (k, f, d)
+    assert first_over is None, ("H/Q leave 1e-10 first at iteration", first_over, "worst", worst)
+
+
+def test_c3_string_iteration_matches_oracle(ps):
+    """C3 at full size: one string iteration of 40 images of 128x128 (three
+    SCFT iterations per image, arc length, spline re-sampling), against the
+    oracle's composition of polystring_AB's steps."""
+    from polystring_b200 import workloads
+    m_img, shape, L = 40, (128, 128, 1), 8.0
+    Ms, chiN, lam = workloads.ms_from(0.35, 128), 18.0, (0.05, 0.05, 5.0)
+    wa, wb = workloads.string_images(m=m_img, shape=shape, L=L)
+    g = ps.StringAB(m_img, 2, shape, ps.make_cell(2, "SQUARE", L), Ms, chiN, lam=lam, max_iter=3)
+    g.set_images(wa, wb)
+    g.iterate(1)
+    o = oracle.ModelAB(2, shape, (L, L), Ms, chiN, lam=lam)
+    wa_o, wb_o = wa.copy(), wb.copy()
+    H = np.zeros(m_img)
+    phiA = np.zeros_like(wa)
+    for s in range(m_img):
+        o.init_fields(wa_o[s], wb_o[s])
+        o.update(3)
+        H[s] = o.H()[0]
+        phiA[s] = o.get("phiA")
+        wa_o[s], wb_o[s] = o.get("wA"), o.get("wB")
+    S = oracle.string_arclength(wa_o)
+    oracle.string_redistribute(wa_o, S, wa[0], wa[-1])
+    oracle.string_redistribute(wb_o, S, wb[0], wb[-1])
+    np.testing.assert_allclose(g.H(), H, rtol=1e-10, atol=0)
+    np.testing.assert_allclose(g.S(), S, rtol=1e-10, atol=1e-12)
+    assert np.abs(g.get("phiA") - phiA).max() < 1e-10
+    assert np.abs(g.get("wa") - wa_o).max() < 1e-10
+    assert np.abs(g.get("wb") - wb_o).max() < 1e-10
+
+
+def test_c5_sample_members_match_oracle(ps):
+    """Every member of the 27-solve uneven sample, advanced as one batch for
+    two Anderson iterations, against its own oracle solve."""
+    from polystring_b200 import workloads
+    specs = workloads.uneven_solves(27)
+    b = ps.BatchAB([dict(dim=3, shape=sp["shape"], cell=ps.make_cell(3, "CUBIC", sp["cell"][1][0]), Ms=sp["Ms"],
+                         chiN=sp["chiN"], lam=sp["lam"], scft=sp["scft"], n_anderson=sp["n_anderson"])
+                    for sp in specs])
+    for k, sp in enumerate(specs):
+        b.set_fields(k, sp["wA"], sp["wB"])
+    b.update(2)
+    for k, sp in enumerate(specs):
+        a = sp["cell"][1][0]
+        o = oracle.ModelAB(3, sp["shape"], (a, a, a), sp["Ms"], sp["chiN"], lam=sp["lam"], scft=sp["scft"],
+                           n_anderson=sp["n_anderson"])
+        o.init_fields(sp["wA"], sp["wB"])
+        o.update(2)
+        Ho, Hg = o.H()[0], b.H(k)[0]
+        assert abs(Hg - Ho) / abs(Ho) < 1e-10, (k, Hg, Ho)
+        for f in ("phiA", "phiB", "wA", "wB"):
+            d = np.abs(b.get(k, f) - o.get(f)).max()
+            assert d < 1e-10, (k, f, d)
+        del o
