@@ -61,6 +61,20 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def fp64_peak_tflops(ps):
+    """FP64 FMA throughput of this GPU measured live (ps_measure_fp64_peak:
+    CUDA events around launches of independent FMA chains on every SM);
+    the nominal 37 TFLOP/s only if the measurement fails."""
+    import ctypes
+    v = ctypes.c_double()
+    try:
+        if ps.lib().ps_measure_fp64_peak(ctypes.byref(v)) == 0 and v.value > 0:
+            return v.value, "measured (ps_measure_fp64_peak, DFMA chains, CUDA events)"
+    except Exception:
+        pass
+    return 37.0, "nominal"
+
+
 def traffic_per_gridpt_step():
     """DRAM bytes per gridpoint-step of the propagator line passes from the
     committed ncu summary (None until one exists)."""
@@ -147,15 +161,47 @@ def cpu_propagation_rate(dim, shape, lengths, Ms, w, seconds, threads):
     return nsteps * M / dt, nsteps, dt
 
 
-def cpu_baseline(cfg, seconds, threads):
-    """Time the CPU oracle on a bounded sample of the workload: RQM4 contour
-    steps of one 64^3 propagator, as many as fit in `seconds` (about 95% of an
-    SCFT iteration is propagation)."""
+def cpu_iteration_rate(cfg, threads, iters, warm=1):
+    """Gridpoint contour steps per second of whole SCFT iterations of the CPU
+    oracle (Model_AB::update restated: four RQM4 propagators, Q, Simpson
+    densities, Anderson mixing) on the workload's seeded fields, `warm`
+    untimed iterations then `iters` timed ones; the same unit the GPU arm
+    times.  Only the oracle's FFTs use the threads."""
+    import oracle
+    oracle.build()
+    oracle.set_threads(threads)
     L = cfg["cell"][1][0]
-    rate, nsteps, dt = cpu_propagation_rate(3, cfg["shape"], (L, L, L), cfg["Ms"], cfg["wA"], seconds, threads)
-    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d RQM4 contour steps of one 64^3 propagator (oracle/scft_oracle.c, own FFT, "
-                      "%d OpenMP threads), %.1f s" % (nsteps, threads, dt)}
+    o = oracle.ModelAB(3, cfg["shape"], (L, L, L), cfg["Ms"], cfg["chiN"], lam=cfg["lam"], mde=cfg["mde"],
+                       scft=cfg["scft"], n_anderson=cfg["n_anderson"])
+    o.init_fields(cfg["wA"], cfg["wB"])
+    o.update(warm)
+    t0 = time.perf_counter()
+    o.update(iters)
+    dt = time.perf_counter() - t0
+    units = 2 * (sum(cfg["Ms"]) - 2) * int(np.prod(cfg["shape"]))
+    return units * iters / dt, dt
+
+
+def cpu_baseline(cfg, threads, iters=2, one_thread_iters=1):
+    """Time the CPU oracle on a bounded sample of the workload: `iters` whole
+    SCFT iterations of the 64^3 model on all host threads, and
+    `one_thread_iters` on one thread (the reference itself is single-threaded)."""
+    rate, dt = cpu_iteration_rate(cfg, threads, iters)
+    out = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": "%d whole SCFT iterations (Model_AB::update: propagators, densities, Anderson) of the 64^3 "
+                     "workload by oracle/scft_oracle.c (own FFT, %d OpenMP threads), %.1f s" % (iters, threads, dt)}
+    if one_thread_iters:
+        r1, dt1 = cpu_iteration_rate(cfg, 1, one_thread_iters)
+        out["one_thread"] = {"value": r1, "unit": UNIT, "cores": 1,
+                             "sample": "%d whole SCFT iteration(s) on one thread, %.1f s" % (one_thread_iters, dt1)}
+    return out
+
+
+def bench_config(cfg, world):
+    """The `config` object both arms print."""
+    return {"workload": WORKLOAD, "grid": list(cfg["shape"]), "Ns": sum(cfg["Ms"]) - 2, "Ms": list(cfg["Ms"]),
+            "step": "one SCFT iteration (Model_AB::update)", "l2_flush": "inputs > L2 (0.8 GB histories)",
+            "parallelism": "replicas" if world > 1 else "single"}
 
 
 def cpu_string_baseline(seconds, threads, m=40, max_iter=3):
@@ -174,7 +220,7 @@ def cpu_string_baseline(seconds, threads, m=40, max_iter=3):
                       "propagation only" % (nsteps, threads, dt)}
 
 
-def cpu_batch_baseline(seconds, threads, n=27):
+def cpu_batch_baseline(seconds, threads, n=256):
     """The uneven batch's CPU leg: the oracle's RQM4 rate on each grid of the
     sample (seconds split between them), applied to every solve's 2 Ns M
     steps, as one host process running the solves one after another would."""
@@ -195,7 +241,7 @@ def cpu_batch_baseline(seconds, threads, n=27):
                       % (threads, ", ".join(samples))}
 
 
-def string_method(ps, iters=10):
+def string_method(ps, fp64=(37.0, "nominal"), iters=10):
     """Secondary result: the batched string method (40 images, 2D 128x128,
     Ns 128, 3 SCFT iterations per image per string iteration) against the
     same SCFT work run image by image through the plain single-model path."""
@@ -231,19 +277,21 @@ def string_method(ps, iters=10):
     return {"config": "C3 string, 40 images 128x128, Ms %s, 3 SCFT iterations per image" % list(Ms),
             "batched_string_iters_per_s": 1.0 / tb, "sequential_plain_gpu_iters_per_s": 1.0 / ts,
             "gridpt_steps_per_s": rate,
-            "fp64": {"flop_per_gridpt_step": flop, "achieved_tflops": rate * flop / 1e12, "peak_tflops": 37.0,
-                     "peak_kind": "nominal", "frac": rate * flop / 37.0e12,
+            "fp64": {"flop_per_gridpt_step": flop, "achieved_tflops": rate * flop / 1e12, "peak_tflops": fp64[0],
+                     "peak_kind": fp64[1], "frac": rate * flop / (fp64[0] * 1e12),
                      "note": "whole string iteration (densities, mixing, spline included) counted as propagation"},
             "speedup_vs_sequential": ts / tb, "launches_per_string_iteration": g.launches_per_iteration(),
             "propagator_path": [l for l in ps.lib().ps_tuning_log().decode().split("\ngrid ") if "128x128x1" in l],
             "timing": "host wall clock around synchronised replays"}
 
 
-def uneven_batch(ps, n=27, iters=2):
-    """Secondary result: C5-style independent solves of uneven grids and Ns
-    (a seeded sample of n solves) advanced as one batch, against the same
-    solves run one after another, each on its own fastest single path
-    (persistent sweeps on these cubic grids).  Device time by CUDA events."""
+def uneven_batch(ps, n=256, iters=2):
+    """Secondary result: the C5 workload -- n = 256 independent solves of
+    uneven grids (32^3, 48^3, 64^3) and Ns (64, 128, 256) -- advanced as one
+    batch for `iters` Anderson iterations (of the 300 the workload runs),
+    against the same solves run one after another, each on its own fastest
+    single path (persistent sweeps on these cubic grids).  Device time by
+    CUDA events."""
     from polystring_b200 import workloads
     specs = workloads.uneven_solves(n)
 
@@ -266,76 +314,61 @@ def uneven_batch(ps, n=27, iters=2):
         ts += m.update_timed(iters)[0] / 1e3
         del m
     sizes = sorted({sp["shape"][0] for sp in specs})
-    return {"config": "C5 sample: %d solves, grids %s^3, Ns 64/128/256, Anderson(10), %d iterations" % (n, sizes, iters),
+    return {"config": "C5: %d solves, grids %s^3, Ns 64/128/256, Anderson(10), %d of 300 iterations timed"
+                      % (n, sizes, iters),
             "batch_gridpt_steps_per_s": work / tb, "sequential_gridpt_steps_per_s": work / ts,
             "speedup_vs_sequential": ts / tb, "launches_per_batch_iteration": launches,
             "timing": "CUDA events on the batch stream / each solve's stream"}
 
 
-def adjoint_c4(ps, iters=120):
+def adjoint_c4(ps, thresh=1e-9, max_iter=4000):
     """Secondary result: the adjoint on C4 (48^3 orthorhombic (3.8, 4.0, 4.2),
-    fA 0.30, chiN 22, Ns 128, seeded start relaxed by Anderson iterations):
-    time of one stress evaluation (dF/dL_cell) and of one loss gradient
-    (Loss = ||phiA - phi_target||^2, phi_target a smoothed seeded field in
-    [0, 1]), each including its forward map, and their agreement with fourth-
-    order central differences of the forward map (h = 1e-4)."""
-    from polystring_b200 import workloads
-    cfg = workloads.config("C4")
-    L = cfg["cell"][1]
-    mk = lambda l: ps.make_cell(3, "ORTHORHOMBIC", *l)
-    m = ps.ModelAB(3, cfg["shape"], mk(L), cfg["Ms"], cfg["chiN"], lam=cfg["lam"], scft="Anderson", n_anderson=20)
+    fA 0.30, chiN 22, Ns 128, seeded noise plus an ordered seed, converged by
+    Anderson mixing to residual `thresh`): time of one stress evaluation
+    (dF/dL_cell) and of one loss gradient (Loss = ||phiA - phi_target||^2,
+    phi_target a smoothed seeded field in [0, 1]), each including its forward
+    map, and their agreement with central differences of the forward map:
+    fourth order at h = 1e-4 and second order at h = 1e-6."""
+    from polystring_b200 import workloads as wl
+    cfg = wl.config("C4")
+    m = wl.model_of(ps, cfg)
     m.set_fields(cfg["wA"], cfg["wB"])
-    m.update(iters)
-    res = m.residual_error()
+    t0 = time.perf_counter()
+    iters, res = wl.converge(m, thresh, max_iter)
+    t_conv = time.perf_counter() - t0
     wA, wB = m.get("wA"), m.get("wB")
-    rng = np.random.default_rng(7)
-    tgt = rng.uniform(0, 1, cfg["shape"])
-    for _ in range(2):                       # smooth the target (periodic 3-point means)
-        tgt = sum(np.roll(tgt, s, ax) for ax in range(3) for s in (-1, 0, 1)) / 9.0
+    tgt = wl.smoothed_target(cfg["shape"])
     m.set_fields(wA, wB)
     st = m.stress()
     t0 = time.perf_counter()
     for _ in range(3):
         st = m.stress()
     t_stress = (time.perf_counter() - t0) / 3
+    st_ck = m.stress(checkpoints=0)
     m.forward()
     phi = m.get("phiA")
     t0 = time.perf_counter()
     for _ in range(3):
         gA, gB = m.grad_w(2.0 * (phi - tgt), np.zeros(cfg["shape"]), 0.0)
     t_grad = (time.perf_counter() - t0) / 3
-    h = 1e-4
-    err_s = 0.0
-    for i in range(3):
-        v = {}
-        for k in (-2, -1, 1, 2):
-            Lp = list(L)
-            Lp[i] += k * h
-            mm = ps.ModelAB(3, cfg["shape"], mk(Lp), cfg["Ms"], cfg["chiN"], lam=cfg["lam"])
-            mm.set_fields(wA, wB)
-            mm.forward()
-            v[k] = -np.log(mm.Q())
-            del mm
-        fd = (v[-2] - 8 * v[-1] + 8 * v[1] - v[2]) / (12 * h)
-        err_s = max(err_s, abs(fd - st[i]))
+    fd4 = [wl.stress_fd(ps, cfg, wA, wB, i, 1e-4, order=4) for i in range(3)]
+    fd2 = [wl.stress_fd(ps, cfg, wA, wB, i, 1e-6, order=2) for i in range(3)]
+    rel = lambda a, b: max(abs(x - y) / abs(y) for x, y in zip(a, b))
+    rng = np.random.default_rng(11)
     dA, dB = rng.standard_normal(cfg["shape"]), rng.standard_normal(cfg["shape"])
-    f = {}
-    for k in (-2, -1, 1, 2):
-        m.set_fields(wA + k * h * dA, wB + k * h * dB)
-        m.forward()
-        f[k] = float(((m.get("phiA") - tgt) ** 2).sum())
-    fd = (f[-2] - 8 * f[-1] + 8 * f[1] - f[2]) / (12 * h)
     an = float((gA * dA).sum() + (gB * dB).sum())
-    m.set_fields(wA, wB)
+    gfd4 = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-4, order=4)
+    gfd2 = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-6, order=2)
     Ns = sum(cfg["Ms"]) - 2
     M = int(np.prod(cfg["shape"]))
-    return {"config": "C4 48^3 orthorhombic (3.8, 4.0, 4.2), Ms %s, %d Anderson iterations (residual %.1e)"
-                      % (list(cfg["Ms"]), iters, res),
-            "stress": list(st), "stress_ms": t_stress * 1e3, "loss_gradient_ms": t_grad * 1e3,
-            "stress_fd_abs_err_max": err_s, "stress_fd_rel_err_max": err_s / max(abs(x) for x in st),
-            "stress_checkpointed": list(m.stress(checkpoints=0)),
-            "gradient_fd_rel_err": abs(fd - an) / abs(an),
-            "fd_note": "4th-order central differences, h = 1e-4; their rounding floor is about 1e-16 |ln Q| / h",
+    return {"config": "C4 48^3 orthorhombic (3.8, 4.0, 4.2), Ms %s, seeded noise + ordered seed, %d Anderson(20) "
+                      "iterations to residual %.1e (%.1f s)" % (list(cfg["Ms"]), iters, res, t_conv),
+            "stress": list(st), "stress_checkpointed": list(st_ck), "checkpointed_rel_diff": rel(st_ck, st),
+            "stress_ms": t_stress * 1e3, "loss_gradient_ms": t_grad * 1e3,
+            "stress_fd4_h1e-4_rel_err_max": rel(st, fd4), "stress_fd2_h1e-6_rel_err_max": rel(st, fd2),
+            "gradient_fd4_h1e-4_rel_err": abs(gfd4 - an) / abs(an),
+            "gradient_fd2_h1e-6_rel_err": abs(gfd2 - an) / abs(an),
+            "fd_note": "central differences of the GPU forward map; loss differences formed point by point",
             "adjoint_gridpt_steps_per_s": Ns * M / t_stress,
             "timing": "host wall clock around synchronised calls (forward map included)"}
 
@@ -414,31 +447,39 @@ def cufft_comparison(ps, cfg, m, reps=3):
 
 
 def run_reference(args, rank, world):
-    """The reference algorithm's CPU restatement on all host threads (rank 0);
-    each step is a bounded sample of the same workload."""
+    """The reference algorithm's CPU restatement on all host threads (rank 0):
+    each step is one whole SCFT iteration of the same workload, the unit the
+    GPU arm times; then one iteration on one thread."""
     if rank != 0:
         return
     cfg = config()
     import oracle
+    oracle.build()
     threads = oracle.max_threads()
-    per = max(1.0, min(20.0, 120.0 / max(1, args.steps)))
-    for _ in range(args.warmup):
-        cpu_baseline(cfg, 0.2, threads)
-    vals = []
-    b = None
-    for _ in range(args.steps):
-        b = cpu_baseline(cfg, per, threads)
-        vals.append(b["value"])
-    v = float(np.median(vals))
+    oracle.set_threads(threads)
+    L = cfg["cell"][1][0]
+    o = oracle.ModelAB(3, cfg["shape"], (L, L, L), cfg["Ms"], cfg["chiN"], lam=cfg["lam"], mde=cfg["mde"],
+                       scft=cfg["scft"], n_anderson=cfg["n_anderson"])
+    o.init_fields(cfg["wA"], cfg["wB"])
+    o.update(max(1, args.warmup))
+    t0 = time.perf_counter()
+    o.update(args.steps)
+    dt = time.perf_counter() - t0
+    del o
     Ns = sum(cfg["Ms"]) - 2
     M = int(np.prod(cfg["shape"]))
+    v = 2 * Ns * M * args.steps / dt
+    r1, dt1 = cpu_iteration_rate(cfg, 1, 1)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2 * Ns * M / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded gyroid + noise fields)",
-            "config": {"workload": WORKLOAD, "grid": list(cfg["shape"]), "Ns": Ns, "l2_flush": "inputs > L2"},
+            "data": "synthetic (seeded gyroid + noise fields)", "config": bench_config(cfg, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": b["sample"] + "; median of %d samples" % args.steps},
+                             "sample": "%d whole SCFT iterations (Model_AB::update) of the 64^3 workload by "
+                                       "oracle/scft_oracle.c (own FFT, %d OpenMP threads) after %d untimed, %.1f s"
+                                       % (args.steps, threads, max(1, args.warmup), dt),
+                             "one_thread": {"value": r1, "unit": UNIT, "cores": 1,
+                                            "sample": "1 whole SCFT iteration on one thread, %.1f s" % dt1}},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -469,6 +510,7 @@ def main():
     m = ps.ModelAB(3, shape, cell, cfg["Ms"], cfg["chiN"], lam=cfg["lam"], mde=cfg["mde"], scft=cfg["scft"],
                    n_anderson=cfg["n_anderson"])
     m.set_fields(cfg["wA"], cfg["wB"])
+    fp64_meas = fp64_peak_tflops(ps)
     m.update(args.warmup)
     m.synchronize()
 
@@ -530,12 +572,13 @@ def main():
     import math
     flop = 15.0 * math.log2(M) + 20.0
     rate = units_per_step * args.steps / prop_s
-    fp64_peak = 37.0e12        # nominal B200 FP64 (not in MEASURED_PEAKS.json)
+    fp64_peak, fp64_kind = fp64_meas
+    fp64_peak *= 1e12
     roof["fp64"] = {"flop_per_gridpt_step": flop, "achieved_tflops": rate * flop / 1e12,
-                    "peak_tflops": fp64_peak / 1e12, "peak_kind": "nominal", "frac": rate * flop / fp64_peak}
+                    "peak_tflops": fp64_peak / 1e12, "peak_kind": fp64_kind, "frac": rate * flop / fp64_peak}
     roof["attainable_frac"] = rate * max(BYTES_PER_GRIDPT_STEP / (peak * 1e9), flop / fp64_peak)
 
-    string = string_method(ps) if rank == 0 and world == 1 else None
+    string = string_method(ps, fp64_meas) if rank == 0 and world == 1 else None
     batch = uneven_batch(ps) if rank == 0 and world == 1 else None
     adj = adjoint_c4(ps) if rank == 0 and world == 1 else None
     cuf = cufft_comparison(ps, cfg, m) if rank == 0 and world == 1 else None
@@ -543,7 +586,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1:
         import oracle
-        cpu = cpu_baseline(cfg, args.cpu_seconds, oracle.max_threads())
+        cpu = cpu_baseline(cfg, oracle.max_threads())
         if string is not None:
             string["cpu_baseline"] = cpu_string_baseline(0.5 * args.cpu_seconds, oracle.max_threads())
         if batch is not None:
@@ -554,8 +597,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded gyroid + noise fields)",
-                "config": {"workload": WORKLOAD, "grid": list(shape), "Ns": Ns, "Ms": list(cfg["Ms"]),
-                           "l2_flush": "inputs > L2 (0.8 GB histories)", "parallelism": "replicas" if world > 1 else "single"},
+                "config": bench_config(cfg, world),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clk.summary(), "H_after": H, "string_method": string, "uneven_batch": batch, "adjoint": adj,
                 "cufft_comparison": cuf}

@@ -92,6 +92,12 @@ const char* ps_version(void);
  * when a model or string context is created; PS_B200_AUTOTUNE=0 disables it. */
 const char* ps_tuning_log(void);
 const char* ps_last_error(void);
+/* FP64 fused multiply-add throughput of the current GPU in TFLOP/s, timed
+ * with CUDA events over a few launches of a kernel of independent FMA chains
+ * on every SM (no counterpart in the reference; the denominator of the FP64
+ * roofline fraction of the propagator sweeps).  Allocates and frees a small
+ * buffer; synchronous. */
+int ps_measure_fp64_peak(double* tflops);
 
 /* ---- propagator updaters (the Updater interface, include/Updater.h:44-69) */
 
@@ -124,8 +130,10 @@ int ps_density_solve_device(int rule, const double* q, const double* qc, int len
  * table lives in a fixed device array compiled into the library, so nothing
  * is allocated.  len (contour points) may not exceed
  * PS_DENSITY_NOALLOC_MAX_LEN; larger values return PS_ERR_INVALID.  The first
- * call on a device looks up the table's device address on the current device;
- * make that first call before any stream capture.  Asynchronous on `stream`.
+ * call on a device looks up the table's device address on the current device
+ * (and the first call after the device's context was reset, which reloads the
+ * library's device code at a new address); make that first call before any
+ * stream capture.  Asynchronous on `stream`.
  * All calls share one table per device: calls whose kernels may overlap on
  * the GPU (different streams with no ordering) race on it. */
 #define PS_DENSITY_NOALLOC_MAX_LEN 8192

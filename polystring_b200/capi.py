@@ -53,6 +53,7 @@ SIGNATURES = [
     ("ps_version", ctypes.c_char_p, []),
     ("ps_tuning_log", ctypes.c_char_p, []),
     ("ps_last_error", ctypes.c_char_p, []),
+    ("ps_measure_fp64_peak", ctypes.c_int, [_dp]),
     ("ps_updater_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(UnitCellC), ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
     ("ps_updater_clone", ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),

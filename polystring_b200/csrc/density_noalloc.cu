@@ -93,21 +93,46 @@ bool rule_valid(int rule, int n) {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_table_mu;
+// per device ordinal: the context the address was looked up in, and the address
+void* g_table_ctx[kMaxDevices] = {};
 double* g_table[kMaxDevices] = {};
 
-// device address of the table on the current device, looked up once per
-// device (the host-side name of the array is not a device address)
+// the calling thread's current driver context (cuCtxGetCurrent, reached
+// through the runtime's driver entry-point table so that the library needs
+// no link against libcuda); nullptr if it cannot be queried
+void* current_context() {
+    typedef int (*CtxGetCurrent)(void**);
+    static CtxGetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (CtxGetCurrent) nullptr;
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// device address of the table on the current device.  The host-side name of
+// the array is not a device address, so it is looked up once per device and
+// context: a cudaDeviceReset (or any other end of the primary context) loads
+// the module again at a new address in the next context, and the changed
+// context handle triggers a new look-up.
 double* table_address() {
     int dev = -1;
     PS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) throw Error(PS_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    void* ctx = current_context();   // null before the runtime has made a context current
     std::lock_guard<std::mutex> lock(g_table_mu);
-    if (!g_table[dev]) {
+    if (!g_table[dev] || !ctx || ctx != g_table_ctx[dev]) {
         double* p = nullptr;
         cudaError_t rc = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), ps_noalloc_contour_weights);
         if (rc != cudaSuccess)
             throw Error(PS_ERR_CUDA, std::string("cudaGetSymbolAddress of the contour table: ") + cudaGetErrorString(rc));
         g_table[dev] = p;
+        g_table_ctx[dev] = current_context();   // current now: the look-up initialised the runtime
     }
     return g_table[dev];
 }

@@ -1,8 +1,12 @@
 """Extract the reference's own known answers for this path into lam_pins.npz.
 
-Run once in a checkout that has the reference tree (the path is given on the
-command line; default /root/reference).  The output is committed so that the
-tests need no access to the reference at run time.
+Run once in a checkout that has the reference tree, whose root is given on
+the command line or in the environment variable POLYSTRING_REFERENCE:
+
+    python tests/golden/make_golden.py <reference root>
+
+The output is committed so that the tests need no access to the reference at
+run time.
 
 What is taken, all from polyorder-master.zip:example/AB/LAM/ (the upstream
 PolyOrder snapshot bundled in the reference):
@@ -28,7 +32,7 @@ import numpy as np
 import scipy.io
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root):
     z = zipfile.ZipFile(os.path.join(ref_root, "polyorder-master.zip"))
     base = "polyorder-master/example/AB/LAM/"
     out = {}
@@ -60,4 +64,7 @@ def main(ref_root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("POLYSTRING_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py <reference root>  (or set POLYSTRING_REFERENCE)")
+    main(root)

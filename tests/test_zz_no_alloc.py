@@ -30,24 +30,37 @@ def _call(lib, fn, rule, q, qc, ds, cc, phi, stream):
                             stream)
 
 
+# (rule, len): every contour rule at the shortest length its precondition
+# allows and at a longer one; consecutive calls change rule and length, so
+# each call must overwrite the previous call's table
+CASES = [("trapezoid", 2), ("trapezoid", 40), ("simpson", 5), ("simpson", 51), ("quad4_closed", 8),
+         ("quad4_closed", 38), ("quad4_open", 10), ("quad4_open", 47), ("quad4_semiopen_left", 9),
+         ("quad4_semiopen_left", 33), ("quad4_semiopen_right", 9), ("quad4_semiopen_right", 60)]
+
+
 def test_noalloc_density_matches_allocating_entry_point_twice(env):
+    """Every rule, each run twice in a row (the first call of a pair follows a
+    call of another rule or length), against the allocating entry point."""
     torch, capi, lib = env
     dev = torch.device("cuda:0")
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     gen = torch.Generator(device="cpu").manual_seed(11)
-    # (rule, len, grid): Simpson on 51 points, then Quad4 closed on 38 points of another grid
-    for rule, length, shape, ds, cc in ((capi.RULES["simpson"], 51, (32, 16, 8), 0.02, 0.7),
-                                        (capi.RULES["quad4_closed"], 38, (24, 12, 10), 0.015, 1.3)):
+    shapes = [(32, 16, 8), (24, 12, 10)]
+    for i, (name, length) in enumerate(CASES):
+        rule = capi.RULES[name]
+        shape = shapes[i % 2]
+        ds, cc = 0.5 / length, 0.7 + 0.1 * i
         q = (1 + 0.1 * torch.randn((length,) + shape, generator=gen, dtype=torch.float64)).to(dev)
         qc = (1 + 0.1 * torch.randn((length,) + shape, generator=gen, dtype=torch.float64)).to(dev)
         ref = torch.zeros(shape, dtype=torch.float64, device=dev)
-        out = torch.full(shape, float("nan"), dtype=torch.float64, device=dev)
         capi.check(_call(lib, "ps_density_solve_device", rule, q, qc, ds, cc, ref, stream))
-        capi.check(_call(lib, "ps_density_solve_device_noalloc", rule, q, qc, ds, cc, out, stream))
-        torch.cuda.synchronize(dev)
-        r, o = ref.cpu().numpy(), out.cpu().numpy()
-        assert np.isfinite(o).all()
-        assert np.abs(o - r).max() < 1e-13, (rule, length)
+        for rep in range(2):
+            out = torch.full(shape, float("nan"), dtype=torch.float64, device=dev)
+            capi.check(_call(lib, "ps_density_solve_device_noalloc", rule, q, qc, ds, cc, out, stream))
+            torch.cuda.synchronize(dev)
+            r, o = ref.cpu().numpy(), out.cpu().numpy()
+            assert np.isfinite(o).all()
+            assert np.abs(o - r).max() < 1e-13, (name, length, rep)
 
 
 def test_noalloc_density_rejects_what_it_cannot_hold(env):
