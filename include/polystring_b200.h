@@ -222,7 +222,8 @@ typedef struct ps_string_ab ps_string_ab;
 /* polystring_AB (scft/polystring_AB.cc:111-152) with m images of the model
  * in p (p->scft must be PS_SCFT_EM: images restart from DATA_INIT fields,
  * Model_AB.cc:52-83) and max_iter SCFT iterations per image per string
- * iteration ([Algorithm_SCFT] max_iter).  3 <= m <= 64. */
+ * iteration ([Algorithm_SCFT] max_iter).  3 <= m <= 64.  H of images outside
+ * a context's shard (ps_string_ab_create_shard) reads as NaN. */
 int ps_string_ab_create(const ps_model_ab_params* p, int m, int max_iter, ps_string_ab** out);
 void ps_string_ab_destroy(ps_string_ab* s);
 /* initial string, m x M per field, image-major (initialize_string,
@@ -240,6 +241,29 @@ int ps_string_ab_S(ps_string_ab* s, double* S);
 int ps_string_ab_get(ps_string_ab* s, int which, double* out);
 int ps_string_ab_synchronize(ps_string_ab* s);
 int ps_string_ab_launches_per_iteration(ps_string_ab* s);
+/* The string with its images partitioned over processes (one per GPU): this
+ * context holds the string fields of all m images but relaxes only images
+ * lo <= s < hi (no counterpart in the reference, whose archived threaded
+ * driver runs one std::thread per image, scft/polystring_AB_back/
+ * polystring_AB_backThread.cc:256-258,412-423).  A sharded string iteration
+ * is ps_string_ab_relax on every rank, an all-gather of the shards' wa and
+ * wb (ps_string_ab_device_ptr), then ps_string_ab_reparameterize on every
+ * rank (the same arithmetic everywhere, so the ranks keep identical strings).
+ * ps_string_ab_iterate is the two in one graph and needs lo = 0, hi = m. */
+int ps_string_ab_create_shard(const ps_model_ab_params* p, int m, int max_iter, int lo, int hi,
+                              ps_string_ab** out);
+/* run_scftInString (polystring_AB.cc:256-281) for the images of the shard:
+ * fresh Yita, max_iter SCFT iterations, H.  Asynchronous on the context's
+ * stream. */
+int ps_string_ab_relax(ps_string_ab* s);
+/* parameterize_string and redistribute_stringBeads (polystring_AB.cc:283-329)
+ * over all m images: arc length, spline re-sampling, ends restored.
+ * Asynchronous on the context's stream. */
+int ps_string_ab_reparameterize(ps_string_ab* s);
+/* device address of the m x M array `which` (0 wa, 1 wb, 2 phiA, 3 phiB) */
+int ps_string_ab_device_ptr(ps_string_ab* s, int which, double** out);
+/* CUDA stream of the context (cudaStream_t as void*) */
+void* ps_string_ab_stream(ps_string_ab* s);
 
 /* ---- independent solves of uneven grids and Ns, advanced together ------- */
 /* The reference runs independent solves one per host thread

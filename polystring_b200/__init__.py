@@ -238,7 +238,7 @@ class StringAB:
     re-sampling, ends restored)."""
 
     def __init__(self, m, dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", max_iter=3,
-                 compressible=False, contour="Simpson"):
+                 compressible=False, contour="Simpson", shard=None):
         Lx, Ly, Lz = shape
         p = capi.ModelABParamsC()
         p.dim, p.Lx, p.Ly, p.Lz = dim, Lx, Ly, Lz
@@ -252,10 +252,18 @@ class StringAB:
         p.compressible = 1 if compressible else 0
         p.contour = capi.CONTOUR[contour.upper()]
         h = ctypes.c_void_p()
-        capi.check(lib().ps_string_ab_create(ctypes.byref(p), int(m), int(max_iter), ctypes.byref(h)))
+        if shard is None:
+            capi.check(lib().ps_string_ab_create(ctypes.byref(p), int(m), int(max_iter), ctypes.byref(h)))
+            self.shard = (0, m)
+        else:
+            lo, hi = shard
+            capi.check(lib().ps_string_ab_create_shard(ctypes.byref(p), int(m), int(max_iter), int(lo), int(hi),
+                                                       ctypes.byref(h)))
+            self.shard = (int(lo), int(hi))
         self._h = h
         self.m = m
         self.shape = tuple(shape)
+        self.M = Lx * Ly * Lz
 
     def set_images(self, wa, wb):
         wa, wb = _f64(wa), _f64(wb)
@@ -264,6 +272,23 @@ class StringAB:
 
     def iterate(self, n=1):
         capi.check(lib().ps_string_ab_iterate(self._h, int(n)))
+
+    def relax(self):
+        """run_scftInString for the images of this context's shard."""
+        capi.check(lib().ps_string_ab_relax(self._h))
+
+    def reparameterize(self):
+        """Arc length, spline re-sampling and ends over all images."""
+        capi.check(lib().ps_string_ab_reparameterize(self._h))
+
+    def device_ptr(self, name):
+        p = ctypes.c_void_p()
+        capi.check(lib().ps_string_ab_device_ptr(self._h, {"wa": 0, "wb": 1, "phiA": 2, "phiB": 3}[name],
+                                                 ctypes.byref(p)))
+        return p.value
+
+    def stream(self):
+        return lib().ps_string_ab_stream(self._h)
 
     def synchronize(self):
         capi.check(lib().ps_string_ab_synchronize(self._h))

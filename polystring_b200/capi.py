@@ -97,6 +97,12 @@ SIGNATURES = [
     ("ps_string_ab_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("ps_string_ab_synchronize", ctypes.c_int, [_vp]),
     ("ps_string_ab_launches_per_iteration", ctypes.c_int, [_vp]),
+    ("ps_string_ab_create_shard", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ps_string_ab_relax", ctypes.c_int, [_vp]),
+    ("ps_string_ab_reparameterize", ctypes.c_int, [_vp]),
+    ("ps_string_ab_device_ptr", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ps_string_ab_stream", _vp, [_vp]),
     ("ps_batch_ab_create", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ps_batch_ab_destroy", None, [_vp]),
     ("ps_batch_ab_set_fields", ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),

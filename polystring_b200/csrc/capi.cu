@@ -292,6 +292,36 @@ int ps_string_ab_create(const ps_model_ab_params* p, int m, int max_iter, ps_str
     });
 }
 
+int ps_string_ab_create_shard(const ps_model_ab_params* p, int m, int max_iter, int lo, int hi, ps_string_ab** out) {
+    return guarded([&] {
+        if (!p || !out) throw Error(PS_ERR_INVALID, "null argument");
+        *out = new ps_string_ab{new StringAB(to_params(p), m, max_iter, lo, hi)};
+    });
+}
+
+int ps_string_ab_relax(ps_string_ab* s) {
+    return guarded([&] {
+        if (!s) throw Error(PS_ERR_INVALID, "null handle");
+        s->ctx->relax();
+    });
+}
+
+int ps_string_ab_reparameterize(ps_string_ab* s) {
+    return guarded([&] {
+        if (!s) throw Error(PS_ERR_INVALID, "null handle");
+        s->ctx->reparameterize();
+    });
+}
+
+int ps_string_ab_device_ptr(ps_string_ab* s, int which, double** out) {
+    return guarded([&] {
+        if (!s || !out) throw Error(PS_ERR_INVALID, "null argument");
+        *out = s->ctx->device_ptr(which);
+    });
+}
+
+void* ps_string_ab_stream(ps_string_ab* s) { return s ? (void*)s->ctx->stream() : nullptr; }
+
 void ps_string_ab_destroy(ps_string_ab* s) {
     if (!s) return;
     delete s->ctx;

@@ -167,8 +167,13 @@ int rgrid(long M) {
 
 }  // namespace
 
-StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), max_iter_(max_iter) {
+StringAB::StringAB(const ModelABParams& p, int m, int max_iter, int lo, int hi)
+    : p_(p), m_(m), max_iter_(max_iter) {
     if (m < 3 || m > kMaxImages) throw Error(-1, "number of images must be in 3.." + std::to_string(kMaxImages));
+    if (hi < 0) hi = m;
+    if (lo < 0 || hi > m || lo >= hi) throw Error(-1, "the shard must be a non-empty range of the images");
+    lo_ = lo;
+    nloc_ = hi - lo;
     if (max_iter < 1) throw Error(-1, "max_iter must be positive");
     if (p.scft != 0) throw Error(-2, "the string method runs simple mixing (DATA_INIT fields)");
     if (p.sA < 2 || p.sB < 2) throw Error(-1, "Ms must be at least [2, 2]");
@@ -186,7 +191,7 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
     if (!contour_weights(ruleA, LA_, cA) || !contour_weights(ruleB, LB_, cB))
         throw Error(-4, "contour quadrature precondition fails");
     PS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    chain_ = new PairChain(p.Lx, p.Ly, p.Lz, p.mde == 1 ? SCHEME_OS2 : SCHEME_RQM4, m);
+    chain_ = new PairChain(p.Lx, p.Ly, p.Lz, p.mde == 1 ? SCHEME_OS2 : SCHEME_RQM4, nloc_);
     if (p.mde == 1) {
         chain_->set_tables(k_laplacian(p_.cell, p.Lx, p.Ly, p.Lz, dsA_), {});
     } else {
@@ -203,7 +208,7 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
         const char* force = getenv("PS_B200_LINE_PASSES");
         if (cluster_sweep_supported(p.Lx, p.Ly, p.Lz) && !(force && force[0] == '1')) {
             use_cluster_ = true;
-            cluster_sweep_prepare(p.Lx, p.Ly, p.Lz, m);
+            cluster_sweep_prepare(p.Lx, p.Ly, p.Lz, nloc_);
             // per-axis factors exp(h k_x^2), exp(h k_y^2) for h = ds, ds/2: the
             // orthogonal k2 along each axis (the other indices 0)
             std::vector<double> kt;
@@ -216,11 +221,11 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
         }
     }
     if (!use_cluster_) chain_->autotune(st_);
-    const size_t mM = (size_t)m * M_;
-    hf_.alloc((size_t)(Ns_ + 1) * mM);
-    hc_.alloc((size_t)(Ns_ + 1) * mM);
-    wa_.alloc(mM); wb_.alloc(mM); yita_.alloc(mM); phiA_.alloc(mM); phiB_.alloc(mM);
-    eFA_.alloc(mM); eHA_.alloc(mM); eFB_.alloc(mM); eHB_.alloc(mM);
+    const size_t mM = (size_t)m * M_, nM = (size_t)nloc_ * M_;
+    hf_.alloc((size_t)(Ns_ + 1) * nM);
+    hc_.alloc((size_t)(Ns_ + 1) * nM);
+    wa_.alloc(mM); wb_.alloc(mM); phiA_.alloc(mM); phiB_.alloc(mM);
+    yita_.alloc(nM); eFA_.alloc(nM); eHA_.alloc(nM); eFB_.alloc(nM); eHB_.alloc(nM);
     ends_.alloc(4 * (size_t)M_);
     cA_.alloc(cA.size()); cB_.alloc(cB.size());
     PS_CUDA(cudaMemcpy(cA_.p, cA.data(), sizeof(double) * cA.size(), cudaMemcpyHostToDevice));
@@ -228,17 +233,21 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter) : p_(p), m_(m), 
     scal_.alloc((size_t)8 * m);
     S_.alloc(m);
     partial_.alloc((size_t)kBG * m * 8);
-    // heads of both chains of every image
-    for (int b = 0; b < m; b++) {
+    // heads of both chains of every image of the shard
+    for (int b = 0; b < nloc_; b++) {
         launch_fill(hf_.p + (size_t)b * (Ns_ + 1) * M_, M_, 1.0, st_);
         launch_fill(hc_.p + (size_t)b * (Ns_ + 1) * M_, M_, 1.0, st_);
     }
     PS_CUDA(cudaMemsetAsync(scal_.p, 0, sizeof(double) * 8 * m, st_));
+    PS_CUDA(cudaMemsetAsync(phiA_.p, 0, sizeof(double) * mM, st_));
+    PS_CUDA(cudaMemsetAsync(phiB_.p, 0, sizeof(double) * mM, st_));
     PS_CUDA(cudaStreamSynchronize(st_));
 }
 
 StringAB::~StringAB() {
     if (giter_) cudaGraphExecDestroy(giter_);
+    if (grelax_) cudaGraphExecDestroy(grelax_);
+    if (grepar_) cudaGraphExecDestroy(grepar_);
     delete chain_;
     if (st_) cudaStreamDestroy(st_);
 }
@@ -255,11 +264,16 @@ void StringAB::set_images(const double* wa, const double* wb, bool dev) {
     PS_CUDA(cudaMemcpyAsync(ends_.p + 3 * M_, wb_.p + (size_t)(m_ - 1) * M_, sizeof(double) * M_, cudaMemcpyDeviceToDevice, st_));
     PS_CUDA(cudaStreamSynchronize(st_));
     iters_ = 0;
+    relaxed_ = false;
     ready_ = true;
 }
 
+// one SCFT iteration (Model_AB::update, EM branch) of the shard's images
 void StringAB::enqueue_scft_iteration() {
     const long hstride = (long)(Ns_ + 1) * M_;
+    const long off = (long)lo_ * M_;
+    double *wa = wa_.p + off, *wb = wb_.p + off, *phiA = phiA_.p + off, *phiB = phiB_.p + off;
+    double* scal = scal_.p + 8 * lo_;
     if (use_cluster_) {
         SweepArgs a{};
         a.hf = hf_.p; a.hc = hc_.p;
@@ -267,44 +281,52 @@ void StringAB::enqueue_scft_iteration() {
         a.ktab = clK_.p;
         a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
         a.bstride_batch = M_; a.bstride_hist = hstride; a.bstride_L = 0;
-        cluster_sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, m_, st_);
+        cluster_sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, nloc_, st_);
     } else {
         LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
         LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
         chain_->enqueue(hf_.p, hc_.p, hstride, Ns_, lf, lc, M_, st_);
     }
     // Q of every image
-    dim3 g(rgrid(M_), m_);
+    dim3 g(rgrid(M_), nloc_);
     breduce_partial<TailMeanF, 1><<<g, kBT, 0, st_>>>(TailMeanF{hf_.p, hstride, (long)Ns_ * M_}, M_, partial_.p);
     PS_CUDA(cudaGetLastError());
-    breduce_final<1><<<m_, kBT, 0, st_>>>(partial_.p, rgrid(M_), 1.0 / (double)M_, scal_.p, 0);
+    breduce_final<1><<<nloc_, kBT, 0, st_>>>(partial_.p, rgrid(M_), 1.0 / (double)M_, scal, 0);
     PS_CUDA(cudaGetLastError());
-    launch_density(hf_.p, hc_.p + (long)LB_ * M_, LA_, M_, cA_.p, dsA_, nullptr, 0.0, phiA_.p, m_, hstride, M_,
-                   scal_.p, st_);
-    launch_density(hf_.p + (long)LA_ * M_, hc_.p, LB_, M_, cB_.p, dsB_, nullptr, 0.0, phiB_.p, m_, hstride, M_,
-                   scal_.p, st_);
+    launch_density(hf_.p, hc_.p + (long)LB_ * M_, LA_, M_, cA_.p, dsA_, nullptr, 0.0, phiA, nloc_, hstride, M_,
+                   scal, st_);
+    launch_density(hf_.p + (long)LA_ * M_, hc_.p, LB_, M_, cB_.p, dsB_, nullptr, 0.0, phiB, nloc_, hstride, M_,
+                   scal, st_);
     EMArgs a{};
-    a.phiA = phiA_.p; a.phiB = phiB_.p; a.wA = wa_.p; a.wB = wb_.p; a.yita = yita_.p;
+    a.phiA = phiA; a.phiB = phiB; a.wA = wa; a.wB = wb; a.yita = yita_.p;
     a.M = M_; a.chiN = p_.chiN; a.lamA = p_.lamA; a.lamB = p_.lamB; a.lamYita = p_.lamYita;
     a.dsA = dsA_; a.dsB = dsB_; a.compressible = p_.compressible;
     a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p; a.bstride = M_;
-    launch_em_update(a, m_, st_);
+    launch_em_update(a, nloc_, st_);
 }
 
-void StringAB::enqueue_string_iteration() {
-    const size_t mM = (size_t)m_ * M_;
-    // resetInString: fresh Yita, Boltzmann factors of the string fields
-    launch_fill(yita_.p, (long)mM, 0.0, st_);
-    launch_factors(wa_.p, wb_.p, M_, dsA_, dsB_, eFA_.p, eHA_.p, eFB_.p, eHB_.p, m_, M_, st_);
+// run_scftInString (polystring_AB.cc:256-281) for the shard's images: fresh
+// Yita and Boltzmann factors of the string fields (resetInString), max_iter
+// SCFT iterations, H = Hw - ln Q per image (Hw into slot 1)
+void StringAB::enqueue_relax() {
+    const long off = (long)lo_ * M_;
+    launch_fill(yita_.p, (long)nloc_ * M_, 0.0, st_);
+    launch_factors(wa_.p + off, wb_.p + off, M_, dsA_, dsB_, eFA_.p, eHA_.p, eFB_.p, eHB_.p, nloc_, M_, st_);
     for (int it = 0; it < max_iter_; it++) enqueue_scft_iteration();
-    // H = Hw - ln Q per image (Hw into slot 1)
-    dim3 g(rgrid(M_), m_);
+    dim3 g(rgrid(M_), nloc_);
     breduce_partial<HwBF, 1><<<g, kBT, 0, st_>>>(
-        HwBF{phiA_.p, phiB_.p, wa_.p, wb_.p, M_, p_.chiN, p_.lamYita, p_.compressible}, M_, partial_.p);
+        HwBF{phiA_.p + off, phiB_.p + off, wa_.p + off, wb_.p + off, M_, p_.chiN, p_.lamYita, p_.compressible}, M_,
+        partial_.p);
     PS_CUDA(cudaGetLastError());
-    breduce_final<1><<<m_, kBT, 0, st_>>>(partial_.p, rgrid(M_), 1.0 / (double)M_, scal_.p, 1);
+    breduce_final<1><<<nloc_, kBT, 0, st_>>>(partial_.p, rgrid(M_), 1.0 / (double)M_, scal_.p + 8 * lo_, 1);
     PS_CUDA(cudaGetLastError());
+}
+
+// parameterize_string and redistribute_stringBeads (polystring_AB.cc:283-329)
+// over all m images
+void StringAB::enqueue_reparameterize() {
     // arc length from wa (slot 2 of image s: mean (wa[s] - wa[s-1])^2)
+    dim3 g(rgrid(M_), m_);
     breduce_partial<ArcBF, 1><<<g, kBT, 0, st_>>>(ArcBF{wa_.p, M_}, M_, partial_.p);
     PS_CUDA(cudaGetLastError());
     breduce_final<1><<<m_, kBT, 0, st_>>>(partial_.p, rgrid(M_), 1.0 / (double)M_, scal_.p, 2);
@@ -323,35 +345,70 @@ void StringAB::enqueue_string_iteration() {
     PS_CUDA(cudaMemcpyAsync(wb_.p + (size_t)(m_ - 1) * M_, ends_.p + 3 * M_, sizeof(double) * M_, cudaMemcpyDeviceToDevice, st_));
 }
 
+void StringAB::enqueue_string_iteration() {
+    enqueue_relax();
+    enqueue_reparameterize();
+}
+
+cudaGraphExec_t StringAB::capture(void (StringAB::*enq)()) {
+    PS_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+        (this->*enq)();
+    } catch (...) {
+        cudaStreamEndCapture(st_, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    PS_CUDA(cudaStreamEndCapture(st_, &g));
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw Error(-3, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return ex;
+}
+
 void StringAB::iterate(int n) {
     if (!ready_) throw Error(-6, "string images are not set");
-    if (!giter_) {
-        PS_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-        cudaGraph_t g = nullptr;
-        try {
-            enqueue_string_iteration();
-        } catch (...) {
-            cudaStreamEndCapture(st_, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-        }
-        PS_CUDA(cudaStreamEndCapture(st_, &g));
-        cudaError_t e = cudaGraphInstantiate(&giter_, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) throw Error(-3, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    }
+    if (nloc_ != m_) throw Error(-6, "a context that relaxes a shard of the images runs relax and reparameterize");
+    if (!giter_) giter_ = capture(&StringAB::enqueue_string_iteration);
     for (int i = 0; i < n; i++) PS_CUDA(cudaGraphLaunch(giter_, st_));
     iters_ += n;
+}
+
+void StringAB::relax() {
+    if (!ready_) throw Error(-6, "string images are not set");
+    if (!grelax_) grelax_ = capture(&StringAB::enqueue_relax);
+    PS_CUDA(cudaGraphLaunch(grelax_, st_));
+    relaxed_ = true;
+}
+
+void StringAB::reparameterize() {
+    if (!ready_) throw Error(-6, "string images are not set");
+    if (!grepar_) grepar_ = capture(&StringAB::enqueue_reparameterize);
+    PS_CUDA(cudaGraphLaunch(grepar_, st_));
+    iters_ += 1;
+}
+
+double* StringAB::device_ptr(int which) {
+    switch (which) {
+    case 0: return wa_.p;
+    case 1: return wb_.p;
+    case 2: return phiA_.p;
+    case 3: return phiB_.p;
+    }
+    throw Error(-1, "unknown string array");
 }
 
 void StringAB::sync() { PS_CUDA(cudaStreamSynchronize(st_)); }
 
 void StringAB::H(double* out) {
-    if (iters_ == 0) throw Error(-6, "no string iteration has run");
+    if (iters_ == 0 && !relaxed_) throw Error(-6, "no string iteration has run");
     std::vector<double> sc((size_t)8 * m_);
     PS_CUDA(cudaMemcpyAsync(sc.data(), scal_.p, sizeof(double) * 8 * m_, cudaMemcpyDeviceToHost, st_));
     PS_CUDA(cudaStreamSynchronize(st_));
-    for (int b = 0; b < m_; b++) out[b] = sc[b * 8 + 1] + (-log(sc[b * 8 + 0]));
+    for (int b = 0; b < m_; b++)   // images outside the shard have no H here
+        out[b] = (b >= lo_ && b < lo_ + nloc_) ? sc[b * 8 + 1] + (-log(sc[b * 8 + 0])) : nan("");
 }
 
 void StringAB::S(double* out) {

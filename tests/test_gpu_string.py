@@ -1,4 +1,6 @@
 """String method on the GPU (all images batched) against the CPU oracle."""
+import os
+
 import numpy as np
 import pytest
 
@@ -117,3 +119,56 @@ def test_cluster_sweep_more_images_than_fit(ps, monkeypatch):
     assert "cluster sweep: 8 CTAs per problem" in log and "batch 64" in log
     np.testing.assert_allclose(out["cluster"][0], out["line_passes"][0], rtol=1e-12, atol=0)
     assert np.abs(out["cluster"][1] - out["line_passes"][1]).max() < 1e-11
+
+
+def test_sharded_contexts_equal_the_whole_string(ps):
+    """Two contexts on one GPU, each relaxing part of the images
+    (ps_string_ab_create_shard), exchanging the relaxed blocks of wa and wb
+    as the ranks' all-gather would, then re-parameterising the whole string:
+    H, S and fields bit-identical to one context running the whole string;
+    and the rank orchestration (string_dist.ShardedString) on one rank equals
+    it too."""
+    import torch
+    from polystring_b200 import workloads
+    from polystring_b200.dist import Ranks
+    from polystring_b200.string_dist import CudaStringBackend, ShardedString
+    m, shape, L = 12, (128, 128, 1), 8.0
+    Ms = workloads.ms_from(0.35, 128)
+    cell = ps.make_cell(2, "SQUARE", L)
+    wa, wb = workloads.string_images(m=m, shape=shape, L=L, seed=6)
+    whole = ps.StringAB(m, 2, shape, cell, Ms, 18.0, max_iter=2)
+    whole.set_images(wa, wb)
+    halves = [CudaStringBackend(ps, m, lo, hi, 2, shape, cell, Ms, 18.0, max_iter=2) for lo, hi in ((0, 5), (5, m))]
+    for h in halves:
+        h.set_images(wa, wb)
+    for it in range(2):
+        whole.iterate(1)
+        for h in halves:
+            h.relax()
+        for h in halves:
+            h.sync()
+        full = {f: torch.cat([h.block(f) for h in halves]).clone() for f in ("wa", "wb")}
+        H = torch.cat([h.H_local() for h in halves]).cpu().numpy()
+        for h in halves:
+            for f in ("wa", "wb"):
+                h.set_all(f, full[f])
+            h.reparameterize()
+            h.sync()
+        assert np.array_equal(H, whole.H()), it
+        for h in halves:
+            assert np.array_equal(h.S(), whole.S()), it
+            assert np.array_equal(h.get("wa"), whole.get("wa")), it
+            assert np.array_equal(h.get("wb"), whole.get("wb")), it
+    for k in ("RANK", "WORLD_SIZE"):
+        os.environ.pop(k, None)
+    st = ShardedString(Ranks(), m, lambda lo, hi: CudaStringBackend(ps, m, lo, hi, 2, shape, cell, Ms, 18.0,
+                                                                      max_iter=2))
+    st.backend.set_images(wa, wb)
+    ref = ps.StringAB(m, 2, shape, cell, Ms, 18.0, max_iter=2)
+    ref.set_images(wa, wb)
+    for it in range(2):
+        H = st.iterate(1)
+        ref.iterate(1)
+        assert np.array_equal(H, ref.H()), it
+        assert np.array_equal(st.S(), ref.S()), it
+        assert np.array_equal(st.backend.get("wa"), ref.get("wa")), it
