@@ -11,7 +11,8 @@
  * a propagator history is len consecutive slices of M (slice s at qs + s*M),
  * as Propagator stores _qs(len, Lx, Ly, Lz) (src/Propagator.cc:12-18).
  * 2D grids use Lz = 1, 1D grids Ly = Lz = 1.  Supported axis lengths: 1, 2,
- * 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256.
+ * 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 352 (= 8 x 4 x 11, the
+ * 128 x 352 grid of the reference's string example).
  *
  * Each context owns its device memory and one CUDA stream; a context is safe
  * to use from one host thread at a time.  "_device" entry points take device

@@ -71,22 +71,26 @@ def build(force=False, verbose=False, jobs=None):
     return LIB
 
 
-HOST_SRC = ["polyorder.cc", "polyorder_b200.cc"]
+# host executables: name -> their own source (each links polyorder.cc too)
+HOST_APPS = {"polyorder_b200": "polyorder_b200.cc", "polystring_ab_b200": "polystring_ab_b200.cc"}
 HOST_EXE = os.path.join(BUILD, "polyorder_b200")
+STRING_EXE = os.path.join(BUILD, "polystring_ab_b200")
 
 
 def build_host(force=False):
-    """The C++ host classes and the polyorder_b200 driver, linked against
-    libpolystring_b200.so (g++, rpath to the library's directory)."""
+    """The C++ host classes and the two drivers (plain SCFT, string method),
+    linked against libpolystring_b200.so (g++, rpath to the library's directory)."""
     host = os.path.join(HERE, "host")
-    srcs = [os.path.join(host, f) for f in HOST_SRC]
-    deps = srcs + [os.path.join(host, "polyorder.h"), LIB] + _headers()
-    if not force and not _needs(HOST_EXE, deps):
-        return HOST_EXE
-    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), "-o", HOST_EXE + ".tmp"] + srcs + \
-        ["-L", BUILD, "-lpolystring_b200", "-Wl,-rpath,$ORIGIN"]
-    subprocess.check_call(cmd)
-    os.replace(HOST_EXE + ".tmp", HOST_EXE)
+    for name, main in HOST_APPS.items():
+        exe = os.path.join(BUILD, name)
+        srcs = [os.path.join(host, "polyorder.cc"), os.path.join(host, main)]
+        deps = srcs + [os.path.join(host, "polyorder.h"), LIB] + _headers()
+        if not force and not _needs(exe, deps):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(HERE, "..", "include"), "-o", exe + ".tmp"] + srcs + \
+            ["-L", BUILD, "-lpolystring_b200", "-Wl,-rpath,$ORIGIN"]
+        subprocess.check_call(cmd)
+        os.replace(exe + ".tmp", exe)
     return HOST_EXE
 
 

@@ -166,7 +166,7 @@ AxisPlan make_axis_plan(int Lx, int Ly, int Lz) {
         if (N <= 1) continue;
         if (!line_size_supported(N))
             throw Error(-2, "unsupported grid size " + std::to_string(N) +
-                                " (supported: 2, 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256)");
+                                " (supported: 2, 4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 352)");
         LineGeom g;
         g.N = N;
         g.S = strides[a];

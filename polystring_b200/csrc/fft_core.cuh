@@ -119,6 +119,45 @@ template <int SIGN> struct Dft<8, SIGN> {
     }
 };
 
+template <int SIGN> struct Dft<11, SIGN> {
+    // Direct 11-point DFT over the symmetric pairs (x[n], x[11 - n]):
+    // X[k], X[11 - k] = x0 + sum_n (x[n] + x[11-n]) cos(2 pi n k / 11)
+    //                  +/- sign i sum_n (x[n] - x[11-n]) sin(2 pi n k / 11), n = 1..5.
+    // cos, sin(2 pi m / 11), m = 1..5, rounded to double from 50-digit values.
+    PS_HD static void run(double2* v) {
+        const double C[5] = {0.84125353283118120551, 0.41541501300188643508, -0.14231483827328514358,
+                             -0.65486073394528510061, -0.95949297361449736865};
+        const double S[5] = {0.54064081745559755543, 0.90963199535451833011, 0.98982144188093268422,
+                             0.75574957435425826890, 0.28173255684142967104};
+        double2 a[5], b[5];
+#pragma unroll
+        for (int n = 1; n <= 5; n++) {
+            a[n - 1] = add(v[n], v[11 - n]);
+            b[n - 1] = sub(v[n], v[11 - n]);
+        }
+        const double2 x0 = v[0];
+        double2 sum = x0;
+#pragma unroll
+        for (int n = 0; n < 5; n++) sum = add(sum, a[n]);
+#pragma unroll
+        for (int k = 1; k <= 5; k++) {
+            double2 t = x0, u = mk(0.0, 0.0);
+#pragma unroll
+            for (int n = 1; n <= 5; n++) {
+                const int m = (n * k) % 11;
+                const double c = m <= 5 ? C[m - 1] : C[10 - m];
+                const double sn = m <= 5 ? S[m - 1] : -S[10 - m];
+                t = mk(t.x + a[n - 1].x * c, t.y + a[n - 1].y * c);
+                u = mk(u.x + b[n - 1].x * sn, u.y + b[n - 1].y * sn);
+            }
+            const double2 iu = mul_si<SIGN>(u);
+            v[k] = add(t, iu);
+            v[11 - k] = sub(t, iu);
+        }
+        v[0] = sum;
+    }
+};
+
 template <int SIGN> struct Dft<16, SIGN> {
     // 16 = 4 x 4: DFT4 over n1 of x[4 n1 + n2], twiddle W16^(n2 k1), DFT4
     // over n2; X[k1 + 4 k2].  W16^m = cos(pi m/8) + sign i sin(pi m/8).
@@ -212,6 +251,7 @@ template <> struct Plan<96>  { static constexpr int P = 3; static constexpr int 
 template <> struct Plan<128> { static constexpr int P = 3; static constexpr int r0 = 8, r1 = 4, r2 = 4; };
 template <> struct Plan<192> { static constexpr int P = 3; static constexpr int r0 = 8, r1 = 8, r2 = 3; };
 template <> struct Plan<256> { static constexpr int P = 3; static constexpr int r0 = 8, r1 = 8, r2 = 4; };
+template <> struct Plan<352> { static constexpr int P = 3; static constexpr int r0 = 8, r1 = 4, r2 = 11; };
 
 // One Stockham butterfly on a tile stored "line fastest": element n of line
 // l sits at buf[n * LP + l] (LP = line pitch).  tw[m] = W_N^m for the

@@ -113,7 +113,7 @@ void launch_n(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaSt
 bool line_size_supported(int N) {
     switch (N) {
     case 2: case 4: case 8: case 12: case 16: case 24: case 32: case 48: case 64:
-    case 96: case 128: case 192: case 256: return true;
+    case 96: case 128: case 192: case 256: case 352: return true;
     default: return false;
     }
 }
@@ -134,6 +134,7 @@ void dispatch(int mode, const LineGeom& g, const StepPtrs& p, int nbatch, cudaSt
     case 128: launch_n<128>(mode, g, p, nbatch, st, po); break;
     case 192: launch_n<192>(mode, g, p, nbatch, st, po); break;
     case 256: launch_n<256>(mode, g, p, nbatch, st, po); break;
+    case 352: launch_n<352>(mode, g, p, nbatch, st, po); break;
     default: throw Error(-2, "unsupported FFT line length " + std::to_string(g.N));
     }
 }

@@ -211,6 +211,37 @@ void tag(const std::vector<char>& b, size_t off, uint32_t& type, uint32_t& nbyte
         total = 8 + ((nbytes + 7) / 8) * 8;
     }
 }
+
+// The values of a numeric data element as doubles.  MATLAB stores an array
+// in the smallest type that holds its values exactly (a double array of
+// small integers as miUINT8, for instance), whatever the array's class, and
+// reads it back as the class; so every numeric storage type is converted.
+bool mat_numeric(uint32_t type, const char* p, uint32_t nbytes, std::vector<double>& v) {
+    auto conv = [&](auto zero) {
+        using T = decltype(zero);
+        const size_t n = nbytes / sizeof(T);
+        v.resize(n);
+        for (size_t i = 0; i < n; i++) {
+            T x;
+            std::memcpy(&x, p + i * sizeof(T), sizeof(T));
+            v[i] = (double)x;
+        }
+        return true;
+    };
+    switch (type) {
+    case 1: return conv(int8_t());
+    case 2: return conv(uint8_t());
+    case 3: return conv(int16_t());
+    case 4: return conv(uint16_t());
+    case 5: return conv(int32_t());
+    case 6: return conv(uint32_t());
+    case 7: return conv(float());
+    case 9: return conv(double());
+    case 12: return conv(int64_t());
+    case 13: return conv(uint64_t());
+    }
+    return false;
+}
 }  // namespace
 
 std::vector<double> mat_read(const std::string& file, const std::string& name, std::vector<int>* dims_out) {
@@ -240,9 +271,10 @@ std::vector<double> mat_read(const std::string& file, const std::string& name, s
             p += tot;
             if (vname == name) {
                 tag(b, p, t, n, d, tot);      // real part
-                if (t != miDOUBLE || p + tot > end) throw std::runtime_error("variable " + name + " is not a double array");
-                std::vector<double> v(n / 8);
-                std::memcpy(v.data(), b.data() + d, n);
+                if (p + tot > end) throw std::runtime_error("truncated variable " + name + " in " + file);
+                std::vector<double> v;
+                if (!mat_numeric(t, b.data() + d, n, v))
+                    throw std::runtime_error("variable " + name + " of " + file + " has no numeric real part");
                 if (dims_out) *dims_out = dims;
                 return v;
             }

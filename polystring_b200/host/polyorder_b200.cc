@@ -4,6 +4,7 @@
 //
 //   polyorder_b200 [param.ini]
 //   polyorder_b200 --check param.ini   (parse only: print the model parameters)
+//   polyorder_b200 --mat file.mat name (print one variable of a MAT-file)
 #include <chrono>
 #include <cstdio>
 #include <iostream>
@@ -37,7 +38,28 @@ static void print_params(const polyorder::Config& cfg) {
     }
 }
 
+// --mat file name: the variable as the MAT-v5 reader returns it (dims, then
+// every value in file order, %.17g)
+static int print_mat(const std::string& file, const std::string& name) {
+    std::vector<int> dims;
+    std::vector<double> v = polyorder::mat_read(file, name, &dims);
+    std::printf("dims");
+    for (int d : dims) std::printf(" %d", d);
+    std::printf("\nvalues");
+    for (double x : v) std::printf(" %.17g", x);
+    std::printf("\n");
+    return 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc > 3 && std::string(argv[1]) == "--mat") {
+        try {
+            return print_mat(argv[2], argv[3]);
+        } catch (const std::exception& e) {
+            std::cerr << "error: " << e.what() << "\n";
+            return 1;
+        }
+    }
     const bool check_only = argc > 1 && std::string(argv[1]) == "--check";
     const std::string file = argc > (check_only ? 2 : 1) ? argv[check_only ? 2 : 1] : "param.ini";
     try {

@@ -15,6 +15,8 @@ PolyOrder snapshot bundled in the reference):
   those example runs (Grid gridInitType = File).
 * {1D,2D}/param.ini: the example config files, copied unchanged to
   lam1d_param.ini and lam2d_param.ini.
+* string/paramString.ini and an excerpt of string/defect.mat (string_files
+  below), for the string application's tests.
 * {1D,2D}/cell_opt_{rqm4,rqm4_anderson,os2,os2_anderson}.mat and
   1D/cell_opt_{etdrk4,etdrk4_anderson}.mat: the (a, F)
   pairs written by scft::save_cell (src/scft.cc:589-609) during the Brent
@@ -25,6 +27,7 @@ PolyOrder snapshot bundled in the reference):
 """
 import io
 import os
+import struct
 import sys
 import zipfile
 
@@ -58,9 +61,52 @@ def main(ref_root):
     for dim in ("1D", "2D"):
         with open(os.path.join(here, "lam%s_param.ini" % dim.lower()), "wb") as f:
             f.write(z.read(base + "%s/param.ini" % dim))
+    string_files(ref_root, here)
     dst = os.path.join(here, "lam_pins.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, sorted(out))
+
+
+def mat_elements(raw):
+    """(offset, length, name) of the top-level data elements of a MAT-v5 file."""
+    out = []
+    off = 128
+    while off + 8 <= len(raw):
+        t, n = struct.unpack("<II", raw[off:off + 8])
+        total = 8 if t >> 16 else 8 + (n + 7) // 8 * 8
+        name = None
+        if t == 14:                     # miMATRIX: flags, dims, then the name
+            p = off + 8 + 16
+            dn = struct.unpack("<I", raw[p + 4:p + 8])[0]
+            p += 8 + (dn + 7) // 8 * 8
+            w0 = struct.unpack("<I", raw[p:p + 4])[0]
+            if w0 >> 16:
+                name = raw[p + 4:p + 4 + (w0 >> 16)].decode()
+            else:
+                nn = struct.unpack("<I", raw[p + 4:p + 8])[0]
+                name = raw[p + 8:p + 8 + nn].decode()
+        out.append((off, total, name))
+        off += total
+    return out
+
+
+def string_files(ref_root, here):
+    """The string application's config, unchanged (string/paramString.ini ->
+    paramString.ini), and an excerpt of its end-state file string/defect.mat:
+    its 128-byte header followed, byte for byte, by the data elements of the
+    variables Q, z, t and incomp.  Those are the variables whose storage the
+    reader must convert: MATLAB wrote the double arrays z and incomp as
+    miUINT8 and t as miUINT16 (the 128 x 352 fields are plain miDOUBLE)."""
+    with open(os.path.join(ref_root, "string", "paramString.ini"), "rb") as f:
+        cfg = f.read()
+    with open(os.path.join(here, "paramString.ini"), "wb") as f:
+        f.write(cfg)
+    with open(os.path.join(ref_root, "string", "defect.mat"), "rb") as f:
+        raw = f.read()
+    keep = {"Q", "z", "t", "incomp"}
+    parts = [raw[:128]] + [raw[o:o + n] for o, n, name in mat_elements(raw) if name in keep]
+    with open(os.path.join(here, "defect_excerpt.mat"), "wb") as f:
+        f.write(b"".join(parts))
 
 
 if __name__ == "__main__":

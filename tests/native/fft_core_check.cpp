@@ -123,7 +123,7 @@ int main() {
     e = fmax(e, run<12, -1>());  e = fmax(e, run<16, -1>());  e = fmax(e, run<24, -1>());
     e = fmax(e, run<32, -1>());  e = fmax(e, run<48, -1>());  e = fmax(e, run<64, -1>());
     e = fmax(e, run<96, -1>());  e = fmax(e, run<128, -1>()); e = fmax(e, run<192, -1>());
-    e = fmax(e, run<256, -1>());
+    e = fmax(e, run<256, -1>()); e = fmax(e, run<352, -1>()); e = fmax(e, run<352, 1>());
     e = fmax(e, run<8, 1>());    e = fmax(e, run<48, 1>());   e = fmax(e, run<64, 1>());
     e = fmax(e, run<128, 1>());  e = fmax(e, run<12, 1>());   e = fmax(e, run<256, 1>());
     e = fmax(e, run<48, -1, Plan16x3>());  e = fmax(e, run<48, 1, Plan16x3>());

@@ -16,5 +16,5 @@ def test_fft_core_all_lengths():
         r = subprocess.run([exe], capture_output=True, text=True)
         assert r.returncode == 0, r.stdout + r.stderr
         lines = [l.split() for l in r.stdout.splitlines()]
-        assert len(lines) >= 19
+        assert len(lines) >= 21
         assert max(float(l[2]) for l in lines) < 1e-14

@@ -66,3 +66,57 @@ def test_driver_without_gpu_fails_cleanly(exe, tmp_path, golden):
     d, _, _ = _case(tmp_path, golden, "1d")
     r = subprocess.run([exe, str(d / "param.ini")], capture_output=True, text=True)
     assert r.returncode == 1 and "error" in r.stderr
+
+
+def _mat_values(exe, path, name):
+    r = subprocess.run([exe, "--mat", path, name], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    v = _parse(r.stdout)
+    return [int(x) for x in v["dims"]], np.array([float(x) for x in v.get("values", [])])
+
+
+def test_mat_reader_on_the_reference_string_file_excerpt(exe):
+    """tests/golden/defect_excerpt.mat holds, byte for byte, the header and
+    four variables of the reference's string/defect.mat, among them the double
+    arrays MATLAB stored as miUINT8 (z, incomp) and miUINT16 (t): the reader
+    returns the values scipy reads, in file (column-major) order."""
+    path = os.path.join(GOLD, "defect_excerpt.mat")
+    ref = scipy.io.loadmat(path)
+    for name in ("Q", "z", "t", "incomp"):
+        dims, vals = _mat_values(exe, path, name)
+        want = np.asarray(ref[name], dtype=np.float64)
+        assert dims == list(want.shape), name
+        assert np.array_equal(vals, want.ravel(order="F")), name
+    r = subprocess.run([exe, "--mat", path, "wA"], capture_output=True, text=True)
+    assert r.returncode == 1 and "not found" in r.stderr
+
+
+@pytest.mark.skipif(not os.environ.get("POLYSTRING_REFERENCE"), reason="POLYSTRING_REFERENCE not set")
+def test_mat_reader_on_the_whole_reference_string_files(exe):
+    """Every variable of the reference's string/defect.mat and string/vLam.mat
+    (the end states of its string example), unchanged, against scipy."""
+    for f in ("defect.mat", "vLam.mat"):
+        path = os.path.join(os.environ["POLYSTRING_REFERENCE"], "string", f)
+        ref = scipy.io.loadmat(path)
+        for name in [k for k in ref if not k.startswith("__")]:
+            dims, vals = _mat_values(exe, path, name)
+            want = np.asarray(ref[name], dtype=np.float64)
+            assert dims == list(want.shape), (f, name)
+            assert np.array_equal(vals, want.ravel(order="F")), (f, name)
+
+
+def test_string_driver_without_gpu_fails_cleanly(tmp_path):
+    """The string application reads the reference's paramString.ini and its
+    end-state files, then needs a device."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from polystring_b200 import build
+    build.build()
+    shutil.copy(os.path.join(GOLD, "paramString.ini"), tmp_path / "paramString.ini")
+    rng = np.random.default_rng(0)
+    for f in ("defect.mat", "vLam.mat"):
+        scipy.io.savemat(str(tmp_path / f), {k: rng.uniform(size=(128, 352)) for k in ("wA", "wB", "phiA", "phiB")})
+    r = subprocess.run([build.STRING_EXE, str(tmp_path / "paramString.ini")], capture_output=True, text=True)
+    assert r.returncode == 1 and "error" in r.stderr
+    assert "Initializing string by two ends" in r.stdout
