@@ -18,12 +18,19 @@
 // registers between hardware cluster barriers, then overwrite the local
 // buffer in place, so each field needs one buffer per CTA.
 //
-// One contour step (RQM4.cc:66-92, same operation order as sweep.cu):
-//   A = e^{-w ds/2} q, B = e^{-w ds/4} q      (row layout)
-//   A <- F^-1 L1 F A, B <- F^-1 L2 F B
-//   u = e^{-w ds/2} A / M  (kept in A's buffer), B <- e^{-w ds/4} (e^{-w ds/4} B / M)
-//   B <- F^-1 L2 F B
-//   q[t+1] = (4 e^{-w ds/4} B / M - u) / 3    -> history, next step's A and B
+// For an orthogonal cell F^-1 exp(-h k^2) F = Dx Dy, two commuting line
+// operators (exp(-h k^2) is the product of the axis factors), so Dy runs on
+// the y lines of the row layout and Dx on the x lines of the column layout.
+// One contour step (RQM4.cc:66-92, the reference's operation order for the
+// pointwise work and the divisions by M):
+//   rows:    A = e^{-w ds/2} q, B = e^{-w ds/4} q;  Dy (full) A, Dy (half) B
+//   -> columns (A, B)
+//   columns: Dx (full) A -> u = e^{-w ds/2} A / M;  Dx (half) B ->
+//            qt = e^{-w ds/4} B / M -> B = e^{-w ds/4} qt;  Dx (half) B
+//   -> rows (B, and u copied)
+//   rows:    Dy (half) B -> q[t+1] = (4 e^{-w ds/4} B / M - u) / 3
+//            -> history, next step's A and B
+// Two cluster transposes a step (four field transposes).
 //
 // No grid barrier and no spin wait: the cluster barrier is a hardware
 // barrier every thread of every CTA of the cluster reaches the same number of
@@ -152,7 +159,7 @@ __device__ __noinline__ void local_pass(int buf, int tw, Ad ad, Epi epi) {
 // outputs are exactly forward butterfly j's inputs (r' = m + (R0 / R1) r).
 // epi(l, n, value) maps the inverse output at n to the forward input.  One
 // load barrier and one store barrier instead of two passes' four.
-template <int N, int R0, int R1, int NL, class Ad, class Epi>
+template <int N, int R0, int R1, int NL, bool LFAST, class Ad, class Epi>
 __device__ __noinline__ void inv_epi_fwd_pass(int buf, int tw, Ad ad, Epi epi) {
     static_assert(R0 * R1 == N && R0 % R1 == 0, "two-pass plan with R1 dividing R0");
     constexpr int Q = R0 / R1;
@@ -164,8 +171,7 @@ __device__ __noinline__ void inv_epi_fwd_pass(int buf, int tw, Ad ad, Epi epi) {
         const int b = threadIdx.x + k * kCT;
         jj[k] = -1;
         if (TOTAL % kCT == 0 || b < TOTAL) {
-            ll[k] = b / R1;
-            jj[k] = b % R1;
+            bmap<NL, R1, LFAST>(b, ll[k], jj[k]);
 #pragma unroll
             for (int m = 0; m < Q; m++)
 #pragma unroll
@@ -297,6 +303,32 @@ __device__ __noinline__ void gather_pass(int buf, Src src, Ad ad) {
     }
 }
 
+// The cluster transpose of a field that needs no transform next (the
+// full-step result u): the values of NL lines of N points come from the
+// peers' buffers (src(l, n)), a cluster barrier orders the reads before any
+// CTA overwrites its buffer, then they are stored in this CTA's layout
+// (ad(l, n)).  With LFAST false consecutive threads take consecutive n.
+template <int N, int NL, bool LFAST, class Src, class Ad>
+__device__ __noinline__ void gather_copy(int buf, Src src, Ad ad) {
+    constexpr int TOTAL = NL * N, BPT = (TOTAL + kCT - 1) / kCT;
+    double2 v[BPT];
+    int ll[BPT], nn[BPT];
+#pragma unroll
+    for (int k = 0; k < BPT; k++) {
+        const int b = threadIdx.x + k * kCT;
+        nn[k] = -1;
+        if (TOTAL % kCT == 0 || b < TOTAL) {
+            bmap<NL, N, LFAST>(b, ll[k], nn[k]);
+            v[k] = *src(ll[k], nn[k]);
+        }
+    }
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < BPT; k++)
+        if (nn[k] >= 0) csm[buf + ad(ll[k], nn[k])] = v[k];
+}
+
 template <int LX, int LY, int C>
 __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
     using G = CGeo<LX, LY, C, kCT>;
@@ -356,57 +388,56 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
                    (n % G::YC);
         };
     };
-    // Forward y transform in row layout, of A and B with their passes
-    // interleaved (each pass's barrier after its loads also orders the other
-    // field's stores before the next pass on that field).  The transposes that
-    // follow start with a cluster barrier.
-    // (after step 0 the first pass was fused into the previous step's end)
-    auto fwd_y2 = [&](bool first_pass) {
-        if (first_pass) {
-            local_pass<LY, Y0, 1, -1, G::XR, true, false>(A, twy, rowAd, NoEpi());
-            local_pass<LY, Y0, 1, -1, G::XR, true, false>(B, twy, rowAd, NoEpi());
-        }
-        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(A, twy, rowAd, NoEpi());
-        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
-    };
-    // x transform, k-space multiply by exp(-k^2 h) (fused into the last forward
-    // pass), inverse x transform, in column layout (the first forward pass was
-    // the gather): A with L1 and B with L2 interleaved, or B alone
-    // (orthogonal cells: exp(h (k_x^2 + k_y^2)) as the product of per-axis
-    // factors kept in shared memory, half = 0 for the full step, 1 for ds/2)
-    auto kmul = [rk](int half) {
-        return [rk, half](int l, int n, double2 v) {
-            const double* kt = reinterpret_cast<const double*>(csm + G::KT) + half * (LX + LY);
-            const double f = kt[n] * kt[LX + rk * G::YC + l];
+    // The diffusion operator F^-1 exp(-h k^2) F of an orthogonal cell is the
+    // product of two commuting line operators, Dy = F_y^-1 exp(-h k_y^2) F_y
+    // on the y lines and Dx on the x lines.  Dy runs in row layout and Dx in
+    // column layout, each as a forward line transform whose last pass
+    // multiplies by the axis factor (kept in shared memory), then an inverse
+    // line transform.  The inverse transforms are unnormalised; the division
+    // by M comes after both, where the reference divides.  A contour step
+    // then needs two cluster transposes (four field transposes) instead of
+    // the four (six) of whole 2D transforms.
+    auto ky = [](int half) {      // row layout: element n of a row is k_y index n
+        return [half](int, int n, double2 v) {
+            const double f = reinterpret_cast<const double*>(csm + G::KT)[half * (LX + LY) + LX + n];
             return make_double2(v.x * f, v.y * f);
         };
     };
-    auto x_prop2 = [&]() {
-        local_pass<LX, X1, X0, -1, G::YC, true, false>(A, twx, colAd, kmul(0));
-        local_pass<LX, X1, X0, -1, G::YC, true, false>(B, twx, colAd, kmul(1));
-        local_pass<LX, X0, 1, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
-        local_pass<LX, X0, 1, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
-        local_pass<LX, X1, X0, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
-        local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+    auto kx = [](int half) {      // column layout: element n of a column is k_x index n
+        return [half](int, int n, double2 v) {
+            const double f = reinterpret_cast<const double*>(csm + G::KT)[half * (LX + LY) + n];
+            return make_double2(v.x * f, v.y * f);
+        };
     };
-    auto x_prop1 = [&]() {
-        local_pass<LX, X1, X0, -1, G::YC, true, true>(B, twx, colAd, kmul(1));
-        local_pass<LX, X0, 1, +1, G::YC, true, true>(B, twx, colAd, NoEpi());
-        local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+    // Dy after its first forward pass: A with the full-step factor, B with the
+    // half-step one, passes interleaved (each pass's load barrier orders the
+    // other field's stores); the last inverse pass leaves the stores to the
+    // cluster barrier of the transpose that follows
+    auto dy2 = [&]() {
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(A, twy, rowAd, ky(0));
+        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, ky(1));
+        local_pass<LY, Y0, 1, +1, G::XR, false, false>(A, twy, rowAd, NoEpi());
+        local_pass<LY, Y0, 1, +1, G::XR, false, false>(B, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, +1, G::XR, false, false>(A, twy, rowAd, NoEpi());
+        local_pass<LY, Y1, Y0, +1, G::XR, false, false>(B, twy, rowAd, NoEpi());
     };
-    // peers' rows -> first x pass -> this CTA's columns (both fields or one)
-    auto rows_to_cols = [&](bool both) {
+    // peers' rows -> first forward x pass -> this CTA's columns, both fields
+    auto rows_to_cols2 = [&]() {
         cl.sync();                                   // every CTA's rows final
         gather_pass<LX, X0, -1, G::YC, true>(B, fromRows(B), colAd);
-        if (both) gather_pass<LX, X0, -1, G::YC, true>(A, fromRows(A), colAd);
+        gather_pass<LX, X0, -1, G::YC, true>(A, fromRows(A), colAd);
         __syncthreads();
     };
-    auto cols_to_rows = [&](bool both) {
+    // peers' columns -> this CTA's rows: B with the first forward y pass, and
+    // A (the full-step result u) copied as it is
+    auto cols_to_rows2 = [&]() {
         cl.sync();                                   // every CTA's columns final
-        gather_pass<LY, Y0, +1, G::XR, false>(B, fromCols(B), rowAd);
-        if (both) gather_pass<LY, Y0, +1, G::XR, false>(A, fromCols(A), rowAd);
+        gather_pass<LY, Y0, -1, G::XR, false>(B, fromCols(B), rowAd);
+        gather_copy<LY, G::XR, false>(A, fromCols(A), rowAd);
         __syncthreads();
     };
+    // global index of element n of local column l (column layout)
+    auto gcol = [rk](int l, int n) -> long { return (long)n * LY + rk * G::YC + l; };
 
     // step 0 inputs: A = e^{-w ds/2} q[0], B = e^{-w ds/4} q[0]
     {
@@ -425,32 +456,42 @@ __global__ void __launch_bounds__(kCT, 3) cluster_sweep2d_kernel(SweepArgs a) {
 
     for (int t = 0; t < a.Ns; t++) {
         const double *ef = eF(0, t), *ec = eF(1, t), *hfp = eH(0, t), *hcp = eH(1, t);
-        // ---- full step (A, L1) and first half step (B, L2) ---------------------
-        fwd_y2(t == 0);
-        rows_to_cols(true);
-        x_prop2();
-        cols_to_rows(true);
-        // last inverse y pass; u = e^{-w ds/2} A / M stays in A,
-        // B <- e^{-w ds/4} (e^{-w ds/4} B / M)
-        local_pass<LY, Y1, Y0, +1, G::XR, false, false>(A, twy, rowAd, [=](int l, int n, double2 v) {
-            const long g = g0 + l * LY + n;
+        // ---- Dy of the full step (A) and of the first half step (B) ----------
+        // (after step 0 the first forward pass was fused into the previous
+        // step's end)
+        if (t == 0) {
+            local_pass<LY, Y0, 1, -1, G::XR, false, false>(A, twy, rowAd, NoEpi());
+            local_pass<LY, Y0, 1, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
+        }
+        dy2();
+        rows_to_cols2();
+        // ---- Dx of both in column layout -------------------------------------
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(A, twx, colAd, kx(0));
+        local_pass<LX, X1, X0, -1, G::YC, true, false>(B, twx, colAd, kx(1));
+        local_pass<LX, X0, 1, +1, G::YC, true, false>(A, twx, colAd, NoEpi());
+        local_pass<LX, X0, 1, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+        // u = e^{-w ds/2} A / M stays in A
+        local_pass<LX, X1, X0, +1, G::YC, true, false>(A, twx, colAd, [=](int l, int n, double2 v) {
+            const long g = gcol(l, n);
             return make_double2(div_pow2_or_rn(v.x * __ldg(ef + g), Md, rMd, mpow2),
                                 div_pow2_or_rn(v.y * __ldg(ec + g), Md, rMd, mpow2));
         });
-        // (B's last inverse pass, its epilogue and the first forward pass of
-        // the second half step in one register-resident pass)
-        inv_epi_fwd_pass<LY, Y0, Y1, G::XR>(B, twy, rowAd, [=](int l, int n, double2 v) {
-            const long g = g0 + l * LY + n;
+        // B's last inverse x pass, qt = e^{-w ds/4} B / M, the second half
+        // step's input e^{-w ds/4} qt and its first forward x pass, in registers
+        inv_epi_fwd_pass<LX, X0, X1, G::YC, true>(B, twx, colAd, [=](int l, int n, double2 v) {
+            const long g = gcol(l, n);
             const double ha = __ldg(hfp + g), hb = __ldg(hcp + g);
             const double qtf = div_pow2_or_rn(v.x * ha, Md, rMd, mpow2);
             const double qtc = div_pow2_or_rn(v.y * hb, Md, rMd, mpow2);
             return make_double2(ha * qtf, hb * qtc);
         });
-        // ---- second half step (B, L2) -------------------------------------------
-        local_pass<LY, Y1, Y0, -1, G::XR, false, false>(B, twy, rowAd, NoEpi());
-        rows_to_cols(false);
-        x_prop1();
-        cols_to_rows(false);
+        // ---- second half step: Dx in column layout, then Dy in row layout ------
+        local_pass<LX, X1, X0, -1, G::YC, true, true>(B, twx, colAd, kx(1));
+        local_pass<LX, X0, 1, +1, G::YC, true, true>(B, twx, colAd, NoEpi());
+        local_pass<LX, X1, X0, +1, G::YC, true, false>(B, twx, colAd, NoEpi());
+        cols_to_rows2();
+        local_pass<LY, Y1, Y0, -1, G::XR, false, true>(B, twy, rowAd, ky(1));
+        local_pass<LY, Y0, 1, +1, G::XR, false, true>(B, twy, rowAd, NoEpi());
         // last inverse y pass fused with q[t+1] = (4 qt2 - u) / 3, the history
         // write and the next step's inputs A = e^{-w ds/2} q, B = e^{-w ds/4} q
         const bool next = t + 1 < a.Ns;

@@ -1,8 +1,6 @@
 // sweep64.cu -- persistent RQM4 sweep specialised for 64^3 grids.
 //
-// Same phase structure as sweep.cu (x-pass | plane | x-pass | plane per
-// contour step, grid barriers in between), built around a register-resident
-// 64 = 8 x 8 four-step FFT:
+// Built around a register-resident 64 = 8 x 8 four-step FFT:
 //
 //   a 64-point line is owned by 8 lanes of one warp; lane t holds the
 //   stride-8 set x[8 n1 + t].  Pass 1 is an 8-point DFT over n1 and the
@@ -10,20 +8,23 @@
 //   a rotation swizzle (element (k1, n2) at slot 8 k1 + ((n2 + k1) & 7), no
 //   bank conflicts) and __syncwarp only; pass 2 is an 8-point DFT over n2,
 //   after which lane t holds X[t + 8 k2] -- again a stride-8 set with offset
-//   t.  So an inverse transform, elementwise work and the next forward
-//   transform chain in registers with no shared-memory round trip.
+//   t.  So a forward transform, the k-space factor and the inverse transform
+//   of one line operator chain in registers, and so do consecutive operators.
 //
-// A 2D (y, z) plane FFT is one sweep over the 64 rows (z lines) and one over
-// the 64 columns (y lines) with a single CTA barrier between them.  x-pass
-// tasks are warp-sized (4 columns) and need no CTA barrier at all.
+// For an orthogonal cell exp(-h k^2) is the product of per-axis factors, so
+// each split step's F^-1 exp(-h k^2) F is a product Dx Dy Dz of commuting
+// line operators.  A contour step is two grid-wide phases with a grid barrier
+// after each: an x-pass over the 4096 (y, z) columns (warp-sized tasks, no CTA
+// barrier) and a plane phase over the 64 x-slabs (Dy and Dz with one transpose
+// through shared memory each way).
 //
 // Plane work is statically mapped: CTA b < 128 owns slab s = b % 64 in role
 // b / 64 for the whole sweep, keeps the slab's e^{-w ds/4} factors of both
 // blocks in shared memory, and prefetches the full-step slab u with a 1D
 // bulk copy (cp.async.bulk, no multicast) completed on an mbarrier.
 // e^{-w ds/2} is formed as (e^{-w ds/4})^2, and the k-space factors as
-// products of per-axis tables; both agree with the reference's direct exp()
-// evaluations to a few ulps.
+// per-axis tables; both agree with the reference's direct exp() evaluations
+// to a few ulps.
 #include "ps_internal.h"
 #include "fft_core.cuh"
 #include "sweep.h"
@@ -32,7 +33,6 @@ namespace ps {
 
 namespace {
 
-constexpr int N64 = 64;
 constexpr int P64 = 64 * 64;          // points per slab
 constexpr long M64 = 64L * 64 * 64;
 constexpr int NT = 512;
@@ -152,104 +152,131 @@ __device__ __forceinline__ void fft64(double2 (&v)[8], int t, double2* line, int
     Dft<8, SIGN>::run(v);
 }
 
-struct S64 {
-    double2* plane;
-    const double* ehA;
-    const double* ehB;
-    double2* u;
-    const double2* tw;
-    const double* tab;   // [0..63] x full, [64..] y full, [128..] z full, [192..] x half, ...
-};
-
-// forward plane FFT: v holds row y = r, z = 8 n1 + t (the z-line input set).
-// Writes the spectrum of the slab to global Zg (natural order).
-__device__ __forceinline__ void plane_forward(double2 (&v)[8], const S64& s, double2* Zg) {
-    const int tid = threadIdx.x, t = tid & 7, r = tid >> 3;
-    double2* row = s.plane + r * PITCH;
-    fft64<-1>(v, t, row, 1, s.tw);
-    __syncwarp();
-#pragma unroll
-    for (int k2 = 0; k2 < 8; k2++) row[t + 8 * k2] = v[k2];
-    __syncthreads();
-    // y lines: column c = r
-    double2* col = s.plane + r;
-#pragma unroll
-    for (int n1 = 0; n1 < 8; n1++) v[n1] = col[(8 * n1 + t) * PITCH];
-    fft64<-1>(v, t, col, PITCH, s.tw);
-#pragma unroll
-    for (int k2 = 0; k2 < 8; k2++) Zg[(t + 8 * k2) * 64 + r] = v[k2];
-    __syncthreads();   // plane buffer is reused by the caller
+// Per-axis k factors in shared memory: tab[h * 192 + axis * 64 + k] =
+// exp(h' ds k_axis^2) for h = 0 (full step) and 1 (half step), axis 0 x, 1 y, 2 z.
+__device__ __forceinline__ const double* ktab(const double* tab, int half, int axis) {
+    return tab + half * 192 + axis * 64;
 }
 
-// inverse plane FFT of the slab spectrum Zg (global, natural order); on exit
-// v holds row y = r, z = t + 8 k2 of the (unnormalised) inverse.
-__device__ __forceinline__ void plane_inverse(double2 (&v)[8], const S64& s, const double2* Zg) {
-    const int tid = threadIdx.x, t = tid & 7, r = tid >> 3;
-    double2* col = s.plane + r;
+// Line operator D = F^-1 diag(L) F of one 64-point line held as the stride-8
+// set of lane t (v[j] = element t + 8 j on entry and on exit); `line` is the
+// line's 64-slot exchange area (stride es), L the axis factor table.
+__device__ __forceinline__ void line_op(double2 (&v)[8], int t, double2* line, int es, const double2* tw,
+                                        const double* L) {
+    fft64<-1>(v, t, line, es, tw);
 #pragma unroll
-    for (int n1 = 0; n1 < 8; n1++) v[n1] = Zg[(8 * n1 + t) * 64 + r];
-    fft64<+1>(v, t, col, PITCH, s.tw);
+    for (int k = 0; k < 8; k++) {
+        const double f = L[t + 8 * k];
+        v[k] = make_double2(v[k].x * f, v[k].y * f);
+    }
     __syncwarp();
-#pragma unroll
-    for (int k2 = 0; k2 < 8; k2++) col[(t + 8 * k2) * PITCH] = v[k2];
-    __syncthreads();
-    double2* row = s.plane + r * PITCH;
-#pragma unroll
-    for (int n1 = 0; n1 < 8; n1++) v[n1] = row[8 * n1 + t];
-    fft64<+1>(v, t, row, 1, s.tw);
-    __syncthreads();   // plane buffer is reused by the caller
+    fft64<+1>(v, t, line, es, tw);
 }
 
-// x-pass of one field over all columns; warp task = 4 columns.
-// half = 0: k table of the full step, 1: of the half step
-__device__ __forceinline__ void xpass(double2* Z, int half, const S64& s, int gwarp, int nwarps) {
-    const int lane = threadIdx.x & 31, t = lane & 7, cq = lane >> 3;
-    double2* scratch = s.plane + (threadIdx.x >> 5) * 256 + cq * 64;
-    const double* tx = s.tab + half * 192;
-    const double* ty = tx + 64;
-    const double* tz = tx + 128;
-    for (int task = gwarp; task < P64 / 4; task += nwarps) {
-        const int c = task * 4 + cq;          // column = (ky, kz) = (c / 64, c % 64)
-        double2 v[8];
+// x-pass task of 4 columns c = (y, z) (8 lanes a column, lane t holds the
+// stride-8 set x = t + 8 j).
+//   Z1 columns: Dx of the full step, then u = e^{-w ds/2} v / M  -> ug
+//   Z2 columns: Dx of the half step, qt = e^{-w ds/4} v / M, the second half
+//               step's input e^{-w ds/4} qt and its Dx                -> Z3
+// ef, ec: e^{-w ds/4} of the two lanes' blocks at this step (global).
+__device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zout, const double* ef,
+                                      const double* ec, double2* scratch, int c, int t, const double2* tw,
+                                      const double* tab, double rMd) {
+    double2 v[8];
+    double hf[8], hc[8];
 #pragma unroll
-        for (int n1 = 0; n1 < 8; n1++) v[n1] = Z[(long)(8 * n1 + t) * P64 + c];
-        fft64<-1>(v, t, scratch, 1, s.tw);
-        const double tyz = ty[c >> 6] * tz[c & 63];
+    for (int j = 0; j < 8; j++) {
+        const long g = (long)(t + 8 * j) * P64 + c;
+        v[j] = Zin[g];
+        hf[j] = __ldg(ef + g);
+        hc[j] = __ldg(ec + g);
+    }
+    if (full) {
+        line_op(v, t, scratch, 1, tw, ktab(tab, 0, 0));
 #pragma unroll
-        for (int k2 = 0; k2 < 8; k2++) {
-            double lv = tx[t + 8 * k2] * tyz;
-            v[k2] = make_double2(v[k2].x * lv, v[k2].y * lv);
+        for (int j = 0; j < 8; j++)
+            Zout[(long)(t + 8 * j) * P64 + c] =
+                make_double2((v[j].x * (hf[j] * hf[j])) * rMd, (v[j].y * (hc[j] * hc[j])) * rMd);
+    } else {
+        line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const double qf = (v[j].x * hf[j]) * rMd, qc = (v[j].y * hc[j]) * rMd;
+            v[j] = make_double2(hf[j] * qf, hc[j] * qc);
         }
         __syncwarp();
-        fft64<+1>(v, t, scratch, 1, s.tw);
+        line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
 #pragma unroll
-        for (int k2 = 0; k2 < 8; k2++) Z[(long)(t + 8 * k2) * P64 + c] = v[k2];
-        __syncwarp();
+        for (int j = 0; j < 8; j++) Zout[(long)(t + 8 * j) * P64 + c] = v[j];
     }
+    __syncwarp();
 }
 
+// Dy then Dz of the slab held in y-line order (thread (r, t): column z = r,
+// y = t + 8 j) -> z-line order (row y = r, z = t + 8 j).  One CTA barrier
+// for the transpose through the plane buffer; a second one before the
+// caller reuses the buffer.
+__device__ __forceinline__ void slab_yz(double2 (&v)[8], double2* plane, int r, int t, const double2* tw,
+                                        const double* tab, int half) {
+    double2* col = plane + r;
+    line_op(v, t, col, PITCH, tw, ktab(tab, half, 1));
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; j++) col[(t + 8 * j) * PITCH] = v[j];
+    __syncthreads();
+    double2* row = plane + r * PITCH;
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = row[8 * j + t];
+    line_op(v, t, row, 1, tw, ktab(tab, half, 2));
+    __syncthreads();
+}
+
+// Dz then Dy of the slab held in z-line order -> y-line order.
+__device__ __forceinline__ void slab_zy(double2 (&v)[8], double2* plane, int r, int t, const double2* tw,
+                                        const double* tab, int half) {
+    double2* row = plane + r * PITCH;
+    line_op(v, t, row, 1, tw, ktab(tab, half, 2));
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; j++) row[t + 8 * j] = v[j];
+    __syncthreads();
+    double2* col = plane + r;
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = col[(8 * j + t) * PITCH];
+    line_op(v, t, col, PITCH, tw, ktab(tab, half, 1));
+    __syncthreads();
+}
+
+// The diffusion operator F^-1 exp(-h k^2) F of an orthogonal cell is the
+// product Dx Dy Dz of commuting line operators (exp(-h k^2) is the product of
+// the per-axis factors), so a contour step needs only two grid-wide phases:
+//
+//   x-pass  (4096 columns): Dx of the full step on Z1 -> u; Dx of the first
+//            half step on Z2, the pointwise e^{-w ds/4} work, Dx of the second
+//            half step -> Z3
+//   plane   (slab x = s): Dy Dz of the second half step on Z3 -> qt2,
+//            q[t+1] = (4 qt2 - u) / 3 -> history; the next step's inputs
+//            e^{-w ds/2} q (role 0) and e^{-w ds/4} q (role 1) with their
+//            Dz Dy -> Z1, Z2
+//
+// The divisions by M come after the last inverse transform of each operator,
+// where the reference divides.
 __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const double* __restrict__ tables) {
     extern __shared__ __align__(128) unsigned char smraw[];
-    S64 s;
-    s.plane = reinterpret_cast<double2*>(smraw + OFF_PLANE);
+    double2* plane = reinterpret_cast<double2*>(smraw + OFF_PLANE);
     double* ehA = reinterpret_cast<double*>(smraw + OFF_EHA);
     double* ehB = reinterpret_cast<double*>(smraw + OFF_EHB);
-    s.ehA = ehA;
-    s.ehB = ehB;
-    s.u = reinterpret_cast<double2*>(smraw + OFF_U);
+    double2* su = reinterpret_cast<double2*>(smraw + OFF_U);
     double2* tw = reinterpret_cast<double2*>(smraw + OFF_TW);
     double* tab = reinterpret_cast<double*>(smraw + OFF_TAB);
     void* mbar = smraw + OFF_MBAR;
-    s.tw = tw;
-    s.tab = tab;
 
     const int tid = threadIdx.x, t = tid & 7, r = tid >> 3;
     const int b = blockIdx.x;
     const bool planar = b < 128;
     const int slab = b & 63, role = b >> 6;
     const long soff = (long)slab * P64;
-    const double Md = (double)M64;
-    const double rMd = 1.0 / Md;   // M = 2^18: multiplying by 1/M rounds exactly like dividing
+    const double rMd = 1.0 / (double)M64;   // M = 2^18: multiplying by 1/M rounds exactly like dividing
     unsigned* ctr = a.bar;
     unsigned bidx = 0;
     unsigned mphase = 0;
@@ -268,106 +295,88 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     // x-pass warp index, CTA-fastest so that a phase's tasks spread over all SMs
     const int gwarp = (tid >> 5) * gridDim.x + b;
     const int nwarps = gridDim.x * (NT / 32);
-    double2* Z1 = a.Z1;
-    double2* Z2 = a.Z2;
-    double2* Z3 = a.Z3;
+    const int lane = tid & 31, cq = lane >> 3;
+    double2* scratch = plane + (tid >> 5) * 256 + cq * 64;
     double2* ug = reinterpret_cast<double2*>(a.uf);   // interleaved (u_f, u_c)
 
     // lane block at step t: lane f is in A for t < LA, lane c in B for t < LB
-    auto eh_f = [&](int st) { return st < a.LA ? s.ehA : s.ehB; };
-    auto eh_c = [&](int st) { return st < a.LB ? s.ehB : s.ehA; };
-    const int zb = r * 64 + t;   // slab index of (y = r, z = t) ; + 8 k of z
+    auto sh_f = [&](int st) { return st < a.LA ? ehA : ehB; };          // slab tables (shared)
+    auto sh_c = [&](int st) { return st < a.LB ? ehB : ehA; };
+    auto gl_f = [&](int st) { return st < a.LA ? a.eHA : a.eHB; };      // whole-grid tables (global)
+    auto gl_c = [&](int st) { return st < a.LB ? a.eHB : a.eHA; };
+    const int zb = r * 64 + t;   // slab index of (y = r, z = t); + 8 j of z
     const int zbe = r * EHP + t; // the same point in the factor tables
 
-    // ---- step 0 forward transforms ----------------------------------------
+    // next step's input of this CTA's role from q (z-line order), its Dz Dy,
+    // stored as Z1 (role 0) or Z2 (role 1)
+    auto next_inputs = [&](double2 (&v)[8], int st) {
+        const double* nf = sh_f(st);
+        const double* nc = sh_c(st);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int ze = zbe + 8 * j;
+            double gf = nf[ze], gc = nc[ze];
+            if (role == 0) { gf *= gf; gc *= gc; }
+            v[j] = make_double2(gf * v[j].x, gc * v[j].y);
+        }
+        slab_zy(v, plane, r, t, tw, tab, role);
+        double2* Zg = (role == 0 ? a.Z1 : a.Z2) + soff;
+#pragma unroll
+        for (int j = 0; j < 8; j++) Zg[(t + 8 * j) * 64 + r] = v[j];
+    };
+
+    // ---- step 0 inputs --------------------------------------------------------
     if (planar) {
-        const double* ef = eh_f(0);
-        const double* ec = eh_c(0);
         double2 v[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int zi = zb + 8 * k, ze = zbe + 8 * k;
-            double hf = ef[ze], hc = ec[ze];
-            if (role == 0) { hf *= hf; hc *= hc; }
-            v[k] = make_double2(hf * a.hf[soff + zi], hc * a.hc[soff + zi]);
-        }
-        plane_forward(v, s, (role == 0 ? Z1 : Z2) + soff);
+        for (int j = 0; j < 8; j++) v[j] = make_double2(a.hf[soff + zb + 8 * j], a.hc[soff + zb + 8 * j]);
+        next_inputs(v, 0);
     }
     if (!grid_sync(ctr, a.err, ++bidx)) return;
 
     for (int st = 0; st < a.Ns; st++) {
-        // ---- x-pass on Z1 (full step) and Z2 (half step) ---------------------
-        {
-            const int half = gwarp & 1;
-            xpass(half ? Z2 : Z1, half, s, gwarp >> 1, nwarps >> 1);
+        // ---- x-pass: Z1 -> u, Z2 -> Z3 (the longer Z2 tasks first) ------------
+        for (int task = gwarp; task < 2 * (P64 / 4); task += nwarps) {
+            const bool full = task >= P64 / 4;
+            const int c = (full ? task - P64 / 4 : task) * 4 + cq;
+            xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, gl_f(st), gl_c(st), scratch, c, t, tw, tab, rMd);
         }
         if (!grid_sync(ctr, a.err, ++bidx)) return;
 
-        // ---- plane: Z1 -> u ; Z2 -> qt -> Z3 ---------------------------------
-        if (planar) {
-            const double* ef = eh_f(st);
-            const double* ec = eh_c(st);
-            double2 v[8];
-            plane_inverse(v, s, (role == 0 ? Z1 : Z2) + soff);
-            if (role == 0) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int zi = zb + 8 * k, ze = zbe + 8 * k;
-                    double hf = ef[ze], hc = ec[ze];
-                    ug[soff + zi] = make_double2((v[k].x * (hf * hf)) * rMd, (v[k].y * (hc * hc)) * rMd);
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int ze = zbe + 8 * k;
-                    double hf = ef[ze], hc = ec[ze];
-                    double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
-                    v[k] = make_double2(hf * qf, hc * qc);
-                }
-                plane_forward(v, s, Z3 + soff);
-            }
-        }
-        if (!grid_sync(ctr, a.err, ++bidx)) return;
-
-        // ---- x-pass on Z3 (half step) -----------------------------------------
-        xpass(Z3, 1, s, gwarp, nwarps);
-        if (!grid_sync(ctr, a.err, ++bidx)) return;
-
-        // ---- plane: Z3 -> q[st+1] = (4 qt2 - u) / 3 -> next Z1 / Z2 ------------
+        // ---- plane: Z3 -> q[st+1] -> next Z1 / Z2 ------------------------------
         const bool next = st + 1 < a.Ns;
         if (planar && (role == 0 || next)) {
             if (tid == 0) {
                 // order earlier generic-proxy accesses (other CTAs' u stores,
-                // this CTA's reads of s.u) before the async-proxy bulk copy
+                // this CTA's reads of su) before the async-proxy bulk copy
                 asm volatile("fence.proxy.async;" ::: "memory");
-                bulk_load(s.u, ug + soff, P64 * 16, mbar);
+                bulk_load(su, ug + soff, P64 * 16, mbar);
             }
-            const double* ef = eh_f(st);
-            const double* ec = eh_c(st);
+            const double* ef = sh_f(st);
+            const double* ec = sh_c(st);
             double2 v[8];
-            plane_inverse(v, s, Z3 + soff);
+            // Z3 in y-line order (column z = r, y = t + 8 j)
+            const double2* Z3 = a.Z3 + soff;
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = Z3[(8 * j + t) * 64 + r];
+            slab_yz(v, plane, r, t, tw, tab, 1);
             if (!mbar_wait(mbar, mphase)) { atomicExch(a.err, 3); }
             mphase ^= 1u;
-            const double* nf = next ? eh_f(st + 1) : ef;
-            const double* nc = next ? eh_c(st + 1) : ec;
             double* of = a.hf + (long)(st + 1) * M64 + soff;
             double* oc = a.hc + (long)(st + 1) * M64 + soff;
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int zi = zb + 8 * k, ze = zbe + 8 * k;
-                double hf = ef[ze], hc = ec[ze];
-                double2 u = s.u[zi];
-                double qf = (v[k].x * hf) * rMd, qc = (v[k].y * hc) * rMd;
+            for (int j = 0; j < 8; j++) {
+                const int zi = zb + 8 * j, ze = zbe + 8 * j;
+                const double hf = ef[ze], hc = ec[ze];
+                const double2 u = su[zi];
+                double qf = (v[j].x * hf) * rMd, qc = (v[j].y * hc) * rMd;
                 qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
                 qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
                 if (role == 0) of[zi] = qf;
                 if (role == 1 || !next) oc[zi] = qc;
-                double gf = nf[ze], gc = nc[ze];
-                if (role == 0) { gf *= gf; gc *= gc; }
-                v[k] = make_double2(gf * qf, gc * qc);
+                v[j] = make_double2(qf, qc);
             }
-            if (next) plane_forward(v, s, (role == 0 ? Z1 : Z2) + soff);
-            __syncthreads();
+            if (next) next_inputs(v, st + 1);
         }
         if (next) {
             if (!grid_sync(ctr, a.err, ++bidx)) return;
