@@ -5,9 +5,13 @@
 #include "field_kernels.h"
 
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace ps {
 
@@ -468,6 +472,10 @@ ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
     if (!use_sweep_ && !use_sweep64_ && !batch_member) chain_->autotune(st_);
+    if (use_sweep_) {
+        sweep_variant_ = sweep_default_variant(p.Lx, p.Ly, p.Lz);
+        if (!batch_member) tune_sweep();
+    }
     PS_CUDA(cudaStreamSynchronize(st_));
     launches_per_prop_ = (use_sweep_ || use_sweep64_) ? 1 : chain_->launches_per_step() * Ns_ + (chain_->plan().naxes > 1 ? 1 : 0);
     launches_per_iter_ = launches_per_prop_ + 2 + 2 + (p.scft == 1 ? 4 : 1);
@@ -516,6 +524,71 @@ void ModelAB::set_fields(const double* wA, const double* wB, bool dev) {
     forward_done_ = false;
 }
 
+// The x-tile variant of the generic persistent sweep for this grid, timed
+// once per device and grid shape in a process (whole sweeps on this solve's
+// buffers, before its fields are set; the variants compute the same values,
+// so the choice only changes the time) and cached.  PS_B200_AUTOTUNE=0
+// keeps the default variant, PS_B200_SWEEP_VARIANT=v forces variant v.
+void ModelAB::tune_sweep() {
+    const char* force = getenv("PS_B200_SWEEP_VARIANT");
+    if (force && force[0] >= '0' && force[0] < '0' + kSweepVariants) {
+        sweep_variant_ = force[0] - '0';
+        return;
+    }
+    const char* at = getenv("PS_B200_AUTOTUNE");
+    if (at && at[0] == '0') return;
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, int> cache;   // (device, Lx, Ly, Lz) -> variant
+    int dev = 0;
+    PS_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, p_.Lx, p_.Ly, p_.Lz);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        sweep_variant_ = it->second;
+        return;
+    }
+    // finite data for the timed sweeps (set_fields overwrites the factors)
+    for (double* f : {eFA_.p, eHA_.p, eFB_.p, eHB_.p}) launch_fill(f, M_, 1.0, st_);
+    const SweepArgs a = sweep_descriptor();
+    cudaEvent_t e0, e1;
+    PS_CUDA(cudaEventCreate(&e0));
+    PS_CUDA(cudaEventCreate(&e1));
+    double best = 1e30;
+    char line[512];
+    int n = std::snprintf(line, sizeof(line), "grid %dx%dx%d persistent sweep, x-tile columns (us per step):",
+                          p_.Lx, p_.Ly, p_.Lz);
+    for (int v = 0; v < kSweepVariants; v++) {
+        auto run = [&]() {
+            PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), st_));
+            sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, st_, v);
+        };
+        run();
+        PS_CUDA(cudaEventRecord(e0, st_));
+        for (int r = 0; r < 3; r++) run();
+        PS_CUDA(cudaEventRecord(e1, st_));
+        PS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const double us = 1e3 * ms / 3.0 / Ns_;
+        if (n > 0 && n < (int)sizeof(line))
+            n += std::snprintf(line + n, sizeof(line) - n, " %d=%.1f", sweep_xtile_columns(p_.Lx, p_.Ly, p_.Lz, v), us);
+        if (us < best) {
+            best = us;
+            sweep_variant_ = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int err = 0;
+    PS_CUDA(cudaMemcpy(&err, swerr_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw Error(-3, "persistent sweep reported an error while it was timed");
+    if (n > 0 && n < (int)sizeof(line))
+        std::snprintf(line + n, sizeof(line) - n, " -> %d\n", sweep_xtile_columns(p_.Lx, p_.Ly, p_.Lz, sweep_variant_));
+    tuning_note(line);
+    cache[key] = sweep_variant_;
+}
+
 SweepArgs ModelAB::sweep_descriptor() const {
     if (!use_sweep_) throw Error(-2, "this solve has no generic persistent sweep");
     SweepArgs a{};
@@ -550,7 +623,7 @@ void ModelAB::enqueue_propagate(cudaStream_t s) {
     if (use_sweep_) {
         const SweepArgs a = sweep_descriptor();
         PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), s));
-        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, s);
+        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, s, sweep_variant_);
         return;
     }
     LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};

@@ -203,6 +203,7 @@ private:
     void enqueue_post() { enqueue_post(st_); }
     void ensure_graphs();
     void init_anderson(const double* wA, const double* wB, bool device_ptrs);
+    void tune_sweep();
     void adjoint_weights(std::vector<double>& wAf, std::vector<double>& wBf) const;
     void ensure_adjoint_buffers(bool spec);
     ModelABParams p_;
@@ -215,6 +216,7 @@ private:
     bool use_sweep_ = false;
     bool use_sweep64_ = false;
     int sweep_grid_ = 0;
+    int sweep_variant_ = 0;              // x-tile variant of the generic sweep (tune_sweep)
     DevBuf swZ_, swU_, swL1_, swL2_, swTab_;
     unsigned* swbar_ = nullptr;
     int* swerr_ = nullptr;

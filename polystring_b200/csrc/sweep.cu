@@ -128,16 +128,17 @@ __device__ __forceinline__ void plane_fft(double2* buf, const double2* twy, cons
 // index in a strided batch, 0 when a describes the problem by its own pointers);
 // NT threads a CTA (the thread count changes which thread computes what, not
 // the arithmetic).
-// x tiles of a single 48^3 solve: 18 columns (128 tiles) rather than 36, so
-// more CTAs share its x passes (step 65 -> 57 us); the shared batch launches
-// keep 36 (they fill the GPU with several solves).  The tile never changes
-// the arithmetic, and shared memory is sized for the larger tile.
-template <int LX, int NT>
-constexpr int xtile_cap() { return (LX == 48 && NT == kNT) ? 1024 : 2048; }
+// XTC caps the elements of an x tile: the single-solve kernel comes in the
+// x-tile variants kXtc (the autotuner times them per grid; a 48^3 solve ran
+// 65 -> 57 us per step with 18-column rather than 36-column tiles, as more
+// CTAs share its x passes); the shared batch launches keep 2048 (they fill the
+// GPU with several solves).  The tile never changes the arithmetic, and shared
+// memory is sized for the largest tile.
+constexpr int kXtc[3] = {512, 1024, 2048};
 
-template <int LX, int LY, int LZ, int NT>
+template <int LX, int LY, int LZ, int NT, int XTC>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
-    using G = Geo<LX, LY, LZ, xtile_cap<LX, NT>()>;
+    using G = Geo<LX, LY, LZ, XTC>;
     constexpr int EPT = (G::PT + NT - 1) / NT;   // plane elements per thread
     extern __shared__ double2 sm[];
     double2* twx = sm;
@@ -365,9 +366,15 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
 }
 
 // a strided batch: problem blockIdx.y at blockIdx.y times the strides of a
-template <int LX, int LY, int LZ>
+template <int LX, int LY, int LZ, int XTC>
 __global__ void __launch_bounds__(kNT, 1) sweep_rqm4_kernel(SweepArgs a) {
-    sweep_body<LX, LY, LZ, kNT>(a, blockIdx.y);
+    sweep_body<LX, LY, LZ, kNT, XTC>(a, blockIdx.y);
+}
+
+template <int LX, int LY, int LZ>
+auto sweep_kernel_of(int variant) {
+    return variant == 0 ? sweep_rqm4_kernel<LX, LY, LZ, kXtc[0]>
+         : variant == 1 ? sweep_rqm4_kernel<LX, LY, LZ, kXtc[1]> : sweep_rqm4_kernel<LX, LY, LZ, kXtc[2]>;
 }
 
 // a batch of independent problems, problem blockIdx.y described by d[blockIdx.y]
@@ -376,7 +383,7 @@ template <int LX, int LY, int LZ>
 // measured on the C5 sample 8.65e9 -> 9.71e9 gridpt*steps/s)
 __global__ void __launch_bounds__(kNTB, 2) sweep_rqm4_desc_kernel(const SweepArgs* __restrict__ d) {
     const SweepArgs a = d[blockIdx.y];
-    sweep_body<LX, LY, LZ, kNTB>(a, 0);
+    sweep_body<LX, LY, LZ, kNTB, 2048>(a, 0);
 }
 
 template <int LX, int LY, int LZ>
@@ -388,14 +395,18 @@ size_t smem_bytes() {
 template <int LX, int LY, int LZ>
 int sweep_prepare_t(int* grid_out) {
     const size_t smem = smem_bytes<LX, LY, LZ>();
-    PS_CUDA(cudaFuncSetAttribute(sweep_rqm4_kernel<LX, LY, LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
     PS_CUDA(cudaFuncSetAttribute(sweep_rqm4_desc_kernel<LX, LY, LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
-    int dev = 0, sms = 0, occ = 0, occ_d = 0;
+    int dev = 0, sms = 0, occ = 1 << 30, occ_d = 0;
     PS_CUDA(cudaGetDevice(&dev));
     PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sweep_rqm4_kernel<LX, LY, LZ>, kNT, smem));
+    for (int v = 0; v < kSweepVariants; v++) {
+        int o = 0;
+        PS_CUDA(cudaFuncSetAttribute(sweep_kernel_of<LX, LY, LZ>(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, sweep_kernel_of<LX, LY, LZ>(v), kNT, smem));
+        occ = o < occ ? o : occ;   // one grid size for every variant
+    }
     PS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, sweep_rqm4_desc_kernel<LX, LY, LZ>, kNTB, smem));
     if (occ < 1 || occ_d < 1) throw Error(-2, "sweep kernel does not fit on an SM");
     grid_out[0] = sms * occ;
@@ -405,7 +416,7 @@ int sweep_prepare_t(int* grid_out) {
 }
 
 template <int LX, int LY, int LZ>
-void sweep_launch_t(SweepArgs a, int grid, int nbatch, cudaStream_t st) {
+void sweep_launch_t(SweepArgs a, int grid, int nbatch, cudaStream_t st, int variant) {
     a.twx = twiddle_table(LX);
     a.twy = twiddle_table(LY);
     a.twz = twiddle_table(LZ);
@@ -419,7 +430,7 @@ void sweep_launch_t(SweepArgs a, int grid, int nbatch, cudaStream_t st) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    PS_CUDA(cudaLaunchKernelEx(&cfg, sweep_rqm4_kernel<LX, LY, LZ>, a));
+    PS_CUDA(cudaLaunchKernelEx(&cfg, sweep_kernel_of<LX, LY, LZ>(variant), a));
 }
 
 template <int LX, int LY, int LZ>
@@ -457,8 +468,19 @@ int sweep_prepare(int Lx, int Ly, int Lz) {
     throw Error(-2, "no persistent sweep for this grid");
 }
 
-void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st) {
-#define PS_X(x, y, z) if (Lx == x && Ly == y && Lz == z) { sweep_launch_t<x, y, z>(a, grid, nbatch, st); return; }
+void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st, int variant) {
+    if (variant < 0 || variant >= kSweepVariants) throw Error(-1, "unknown sweep variant");
+#define PS_X(x, y, z) if (Lx == x && Ly == y && Lz == z) { sweep_launch_t<x, y, z>(a, grid, nbatch, st, variant); return; }
+    PS_SWEEP_SHAPES(PS_X)
+#undef PS_X
+    throw Error(-2, "no persistent sweep for this grid");
+}
+
+int sweep_default_variant(int Lx, int Ly, int Lz) { return Lx == 48 ? 1 : 2; }
+
+int sweep_xtile_columns(int Lx, int Ly, int Lz, int variant) {
+#define PS_X(a, b, c) if (Lx == a && Ly == b && Lz == c) { \
+        return variant == 0 ? Geo<a, b, c, kXtc[0]>::XT : variant == 1 ? Geo<a, b, c, kXtc[1]>::XT : Geo<a, b, c, kXtc[2]>::XT; }
     PS_SWEEP_SHAPES(PS_X)
 #undef PS_X
     throw Error(-2, "no persistent sweep for this grid");

@@ -29,7 +29,13 @@ int sweep64_prepare();
 void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStream_t st);
 // sets kernel attributes, builds twiddles; returns the cooperative grid size
 int sweep_prepare(int Lx, int Ly, int Lz);
-void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st);
+// x-tile variants of the single-solve sweep (same arithmetic, different
+// tile widths): the autotuner's choices; sweep_default_variant is the one used
+// untuned; sweep_xtile_columns the columns of an x tile of a variant
+constexpr int kSweepVariants = 3;
+int sweep_default_variant(int Lx, int Ly, int Lz);
+int sweep_xtile_columns(int Lx, int Ly, int Lz, int variant);
+void sweep_launch(const SweepArgs& a, int Lx, int Ly, int Lz, int grid, int nbatch, cudaStream_t st, int variant);
 // Independent problems of one shape in one cooperative launch: d (device
 // memory) holds n descriptors with their own pointers (batch strides 0, bar =
 // 32 zeroed words each), per CTAs work on each problem (per * n must not

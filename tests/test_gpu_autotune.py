@@ -62,3 +62,35 @@ def test_tiles_alone_change_nothing():
     for key in ("(128, 128, 1)", "(48, 32, 24)"):
         assert tuned[key]["H"] == plain[key]["H"]
         assert np.array_equal(np.array(tuned[key]["phiA"]), np.array(plain[key]["phiA"]))
+
+
+@pytest.fixture(scope="module")
+def ps():
+    import polystring_b200
+    return polystring_b200
+
+
+@pytest.mark.parametrize("shape,L", [((32, 32, 32), 3.9), ((48, 48, 48), 4.3)])
+def test_sweep_tile_variants_are_bit_identical(ps, monkeypatch, shape, L):
+    """The x-tile variants of the generic persistent sweep (the autotuner's
+    choices for 32^3 and 48^3) give bit-identical iterations; the tuner logs
+    its timings and choice."""
+    rng = np.random.default_rng(5)
+    wA = 0.5 * rng.uniform(-1, 1, shape)
+    wB = -wA + 0.1 * rng.uniform(-1, 1, shape)
+    out = []
+    for v in ("0", "1", "2"):
+        monkeypatch.setenv("PS_B200_SWEEP_VARIANT", v)
+        m = ps.ModelAB(3, shape, ps.make_cell(3, "CUBIC", L), (13, 21), 20.0, scft="Anderson", n_anderson=3)
+        assert m.launches_per_propagate() == 1
+        m.set_fields(wA, wB)
+        m.update(3)
+        out.append((m.H(), m.get("phiA"), m.get("wB")))
+    for H, phi, w in out[1:]:
+        assert H == out[0][0]
+        assert np.array_equal(phi, out[0][1]) and np.array_equal(w, out[0][2])
+    monkeypatch.delenv("PS_B200_SWEEP_VARIANT")
+    monkeypatch.setenv("PS_B200_AUTOTUNE", "1")
+    ps.ModelAB(3, shape, ps.make_cell(3, "CUBIC", L), (13, 21), 20.0)
+    log = ps.lib().ps_tuning_log().decode()
+    assert "grid %dx%dx%d persistent sweep, x-tile columns" % shape in log
