@@ -198,8 +198,28 @@ def run_once(name):
     """One pass of a case through the library, for profilers and smoke runs:
     'string' (C3: 40 images of 128^2, one string iteration with one SCFT
     iteration per image), 'batch' (nine C5 solves, one batch iteration),
-    'adjoint' (48^3 C4 shape, one stress evaluation)."""
+    'adjoint' (48^3 C4 shape, one stress evaluation); and two small cases
+    for kernel captures, with inputs above the 126 MB L2 but few GB on the
+    device: 'sweep64' (the C2 64^3 model with Ms [21, 41], 244 MB of
+    histories, three iterations: one 64^3 sweep launch each) and 'string12'
+    (12 images of 128^2, Ns 128, three string iterations of one SCFT
+    iteration each: one cluster-sweep launch each)."""
     import polystring_b200 as ps
+    if name == "sweep64":
+        c = config("C2")
+        m = ps.ModelAB(3, c["shape"], ps.make_cell(3, "CUBIC", 4.2), (21, 41), c["chiN"], scft="Anderson",
+                       n_anderson=5)
+        m.set_fields(c["wA"], c["wB"])
+        m.update(3)
+        m.synchronize()
+        return m.H()
+    if name == "string12":
+        g = ps.StringAB(12, 2, (128, 128, 1), ps.make_cell(2, "SQUARE", 8.0), ms_from(0.35, 128), 18.0, max_iter=1)
+        wa, wb = string_images(m=12)
+        g.set_images(wa, wb)
+        g.iterate(3)
+        g.synchronize()
+        return g.H()
     if name == "string":
         g = ps.StringAB(40, 2, (128, 128, 1), ps.make_cell(2, "SQUARE", 8.0), ms_from(0.35, 128), 18.0, max_iter=1)
         wa, wb = string_images(m=40)
