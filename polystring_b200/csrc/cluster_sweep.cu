@@ -308,6 +308,9 @@ __device__ __noinline__ void gather_pass(int buf, Src src, Ad ad) {
 // peers' buffers (src(l, n)), a cluster barrier orders the reads before any
 // CTA overwrites its buffer, then they are stored in this CTA's layout
 // (ad(l, n)).  With LFAST false consecutive threads take consecutive n.
+// Unlike gather_pass, nothing consumes the loaded values before the barrier,
+// so the loads may still be in flight when a thread arrives: the arrival
+// has release semantics (not relaxed), which orders them before it.
 template <int N, int NL, bool LFAST, class Src, class Ad>
 __device__ __noinline__ void gather_copy(int buf, Src src, Ad ad) {
     constexpr int TOTAL = NL * N, BPT = (TOTAL + kCT - 1) / kCT;
@@ -322,8 +325,8 @@ __device__ __noinline__ void gather_copy(int buf, Src src, Ad ad) {
             v[k] = *src(ll[k], nn[k]);
         }
     }
-    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
-    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 #pragma unroll
     for (int k = 0; k < BPT; k++)
         if (nn[k] >= 0) csm[buf + ad(ll[k], nn[k])] = v[k];
