@@ -321,14 +321,15 @@ def uneven_batch(ps, n=256, iters=2):
             "timing": "CUDA events on the batch stream / each solve's stream"}
 
 
-def adjoint_c4(ps, thresh=1e-9, max_iter=4000):
+def adjoint_c4(ps, thresh=1e-9, max_iter=2000):
     """Secondary result: the adjoint on C4 (48^3 orthorhombic (3.8, 4.0, 4.2),
     fA 0.30, chiN 22, Ns 128, seeded noise plus an ordered seed, converged by
     Anderson mixing to residual `thresh`): time of one stress evaluation
     (dF/dL_cell) and of one loss gradient (Loss = ||phiA - phi_target||^2,
     phi_target a smoothed seeded field in [0, 1]), each including its forward
     map, and their agreement with central differences of the forward map:
-    fourth order at h = 1e-4 and second order at h = 1e-6."""
+    fourth order at h = 1e-4 (stress) or 1e-3 (loss) and second order at
+    h = 1e-6."""
     from polystring_b200 import workloads as wl
     cfg = wl.config("C4")
     m = wl.model_of(ps, cfg)
@@ -354,10 +355,13 @@ def adjoint_c4(ps, thresh=1e-9, max_iter=4000):
     fd4 = [wl.stress_fd(ps, cfg, wA, wB, i, 1e-4, order=4) for i in range(3)]
     fd2 = [wl.stress_fd(ps, cfg, wA, wB, i, 1e-6, order=2) for i in range(3)]
     rel = lambda a, b: max(abs(x - y) / abs(y) for x, y in zip(a, b))
-    rng = np.random.default_rng(11)
-    dA, dB = rng.standard_normal(cfg["shape"]), rng.standard_normal(cfg["shape"])
+    # direction: the gradient modulated by a smooth seeded field (a large
+    # projection on the gradient, so the check is not a cancellation)
+    sc = max(np.abs(gA).max(), np.abs(gB).max())
+    mod = 1.0 + wl.smoothed_target(cfg["shape"], seed=21)
+    dA, dB = gA * mod / sc, gB * mod / sc
     an = float((gA * dA).sum() + (gB * dB).sum())
-    gfd4 = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-4, order=4)
+    gfd4 = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-3, order=4)
     gfd2 = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-6, order=2)
     Ns = sum(cfg["Ms"]) - 2
     M = int(np.prod(cfg["shape"]))
@@ -366,7 +370,7 @@ def adjoint_c4(ps, thresh=1e-9, max_iter=4000):
             "stress": list(st), "stress_checkpointed": list(st_ck), "checkpointed_rel_diff": rel(st_ck, st),
             "stress_ms": t_stress * 1e3, "loss_gradient_ms": t_grad * 1e3,
             "stress_fd4_h1e-4_rel_err_max": rel(st, fd4), "stress_fd2_h1e-6_rel_err_max": rel(st, fd2),
-            "gradient_fd4_h1e-4_rel_err": abs(gfd4 - an) / abs(an),
+            "gradient_fd4_h1e-3_rel_err": abs(gfd4 - an) / abs(an),
             "gradient_fd2_h1e-6_rel_err": abs(gfd2 - an) / abs(an),
             "fd_note": "central differences of the GPU forward map; loss differences formed point by point",
             "adjoint_gridpt_steps_per_s": Ns * M / t_stress,

@@ -158,44 +158,47 @@ def test_checkpointed_stress_equals_full_history_stress(ps, dim, shape, cell, Ms
 def test_c4_full_size_adjoint(ps):
     """The adjoint at the full C4 size: 48^3 orthorhombic (3.8, 4.0, 4.2),
     fA 0.30, chiN 22, Ns 128 (Ms [39, 91]), fields converged by Anderson
-    mixing from the seeded start (noise plus an ordered seed).
+    mixing (residual 1e-9) from the seeded start (noise plus an ordered
+    seed), an ordered structure whose stress is 5e-4..7e-3 in every axis.
 
     * stress with the full history and with sqrt(Ns) checkpoints agree to
       1e-10;
     * the stress agrees with fourth-order central differences of -ln Q
-      (h = 1e-4) to 1e-7 relative per component, and with second-order
-      central differences at h = 1e-6 within their rounding floor
-      (~1e-15 |ln Q| / h);
+      (h = 1e-4) to 1e-7 relative per component, and with second-order ones
+      at h = 1e-6 to their rounding floor (~1e-15 |ln Q| / h ~ 1e-9);
     * dLoss/dw for Loss = ||phiA - phi_target||^2 agrees with fourth-order
-      central differences along seeded directions to 1e-8 relative;
+      central differences (h = 1e-3) to 1e-8 relative, along the gradient and
+      along the gradient modulated by a smooth seeded field (directions with
+      a large projection on the gradient, so the check is not a cancellation);
     * d(-ln Q)/dwA = phiA / M to the contour rule's accuracy."""
     from polystring_b200 import workloads as wl
     cfg = wl.config("C4")
     m = wl.model_of(ps, cfg)
     m.set_fields(cfg["wA"], cfg["wB"])
-    it, res = wl.converge(m, 1e-9, 4000)
-    assert res < 1e-7, (it, res)
+    it, res = wl.converge(m, 1e-9, 2000)
+    assert res < 1e-8, (it, res)
     wA, wB = m.get("wA"), m.get("wB")
+    assert np.ptp(m.get("phiA")) > 0.5          # ordered, not the disordered saddle
     m.set_fields(wA, wB)
     st = m.stress()
     ck = m.stress(checkpoints=0)
-    assert np.abs(st).min() > 1e-4, st          # an ordered structure, not the disordered saddle
+    assert np.abs(st).min() > 1e-4, st
     for i in range(3):
         assert abs(ck[i] - st[i]) <= 1e-10 * abs(st[i]), (i, ck[i], st[i])
         fd4 = wl.stress_fd(ps, cfg, wA, wB, i, 1e-4, order=4)
         assert abs(fd4 - st[i]) <= 1e-7 * abs(st[i]), (i, fd4, st[i])
         fd2 = wl.stress_fd(ps, cfg, wA, wB, i, 1e-6, order=2)
-        assert abs(fd2 - st[i]) <= 1e-6 * abs(st[i]), (i, fd2, st[i])
+        assert abs(fd2 - st[i]) <= 1e-6 * np.abs(st).max(), (i, fd2, st[i])
     tgt = wl.smoothed_target(cfg["shape"])
     m.forward()
     phiA, Q = m.get("phiA"), m.Q()
     gA, gB = m.grad_w(2.0 * (phiA - tgt), np.zeros(cfg["shape"]), 0.0)
-    rng = np.random.default_rng(11)
-    for trial in range(2):
-        dA, dB = rng.standard_normal(cfg["shape"]), rng.standard_normal(cfg["shape"])
-        fd = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-4)
+    sc = max(np.abs(gA).max(), np.abs(gB).max())
+    mod = 1.0 + wl.smoothed_target(cfg["shape"], seed=21)
+    for dA, dB in ((gA / sc, gB / sc), (gA * mod / sc, gB * mod / sc)):
+        fd = wl.loss_fd(m, wA, wB, dA, dB, tgt, 1e-3)
         an = float((gA * dA).sum() + (gB * dB).sum())
-        assert abs(fd - an) <= 1e-8 * abs(an), (trial, fd, an)
+        assert abs(fd - an) <= 1e-8 * abs(an), (fd, an)
     m.forward()
     M = np.prod(cfg["shape"])
     lA, lB = m.grad_w(np.zeros(cfg["shape"]), np.zeros(cfg["shape"]), -1.0 / Q)
