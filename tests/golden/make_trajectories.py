@@ -46,7 +46,7 @@ def lengths(cfg):
     return tuple(a)
 
 
-def run(name, n_iter, every=50, n_sample=512):
+def run(name, n_iter, every=50, n_sample=512, suffix=""):
     cfg = workloads.config(name)
     oracle.set_threads(oracle.max_threads())
     o = oracle.ModelAB(cfg["dim"], cfg["shape"], lengths(cfg), cfg["Ms"], cfg["chiN"], lam=cfg["lam"],
@@ -68,7 +68,7 @@ def run(name, n_iter, every=50, n_sample=512):
                 snaps[f].append(a[idx])
                 maxabs[f].append(np.abs(a).max())
             print("%s it %d H %.15f res %.3e (%.0f s)" % (name, k, H, scal[k - 1, 4], time.time() - t0), flush=True)
-            save(name, scal[:k], idx, every, snaps, maxabs)
+            save(name + suffix, scal[:k], idx, every, snaps, maxabs)
     print("done in %.0f s" % (time.time() - t0))
 
 
@@ -85,6 +85,10 @@ def save(name, scal, idx, every, snaps, maxabs):
 
 
 if __name__ == "__main__":
+    # make_trajectories.py NAME [ITERATIONS [EVERY [SUFFIX]]]: the fixture is
+    # tests/golden/<name><suffix>_trajectory.npz
     name = sys.argv[1] if len(sys.argv) > 1 else "C2"
     n = int(sys.argv[2]) if len(sys.argv) > 2 else dict(C1=500, C2=1000).get(name, 100)
-    run(name, n, every=50 if name == "C1" else 100)
+    every = int(sys.argv[3]) if len(sys.argv) > 3 else (50 if name == "C1" else 100)
+    suffix = sys.argv[4] if len(sys.argv) > 4 else ""
+    run(name, n, every=every, suffix=suffix)
