@@ -19,6 +19,8 @@ struct SweepArgs {
     long bstride_hist;               // per-problem stride of the histories
     long bstride_L;                  // per-problem stride of the k tables (0: shared)
     const double* ktab;              // cluster sweep: per-axis exp(h k_x^2), exp(h k_y^2), h = ds then ds/2
+    double2* eHAB;                   // 64^3 sweep: (e^{-w ds/4} of block A, of block B) per point, M
+                                     // pairs, written by the sweep's prologue for its x-pass
 };
 
 bool sweep_supported(int Lx, int Ly, int Lz);

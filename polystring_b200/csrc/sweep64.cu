@@ -178,9 +178,11 @@ __device__ __forceinline__ void line_op(double2 (&v)[8], int t, double2* line, i
 //   Z1 columns: Dx of the full step, then u = e^{-w ds/2} v / M  -> ug
 //   Z2 columns: Dx of the half step, qt = e^{-w ds/4} v / M, the second half
 //               step's input e^{-w ds/4} qt and its Dx                -> Z3
-// ef, ec: e^{-w ds/4} of the two lanes' blocks at this step (global).
-__device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zout, const double* ef,
-                                      const double* ec, double2* scratch, int c, int t, const double2* tw,
+// eAB: (e^{-w ds/4} of block A, of block B) per point; fB, cB: whether lane f
+// and lane c are in block B at this step.  One 16-byte load gives both lanes'
+// factors of a point.
+__device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zout, const double2* eAB,
+                                      bool fB, bool cB, double2* scratch, int c, int t, const double2* tw,
                                       const double* tab, double rMd) {
     double2 v[8];
     double hf[8], hc[8];
@@ -188,8 +190,9 @@ __device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zo
     for (int j = 0; j < 8; j++) {
         const long g = (long)(t + 8 * j) * P64 + c;
         v[j] = Zin[g];
-        hf[j] = __ldg(ef + g);
-        hc[j] = __ldg(ec + g);
+        const double2 e = __ldg(eAB + g);
+        hf[j] = fB ? e.y : e.x;
+        hc[j] = cB ? e.y : e.x;
     }
     if (full) {
         line_op(v, t, scratch, 1, tw, ktab(tab, 0, 0));
@@ -285,8 +288,10 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     for (int i = tid; i < 6 * 64; i += NT) tab[i] = tables[i];
     if (planar) {
         for (int i = tid; i < P64; i += NT) {
-            ehA[(i >> 6) * EHP + (i & 63)] = a.eHA[soff + i];
-            ehB[(i >> 6) * EHP + (i & 63)] = a.eHB[soff + i];
+            const double fa = a.eHA[soff + i], fb = a.eHB[soff + i];
+            ehA[(i >> 6) * EHP + (i & 63)] = fa;
+            ehB[(i >> 6) * EHP + (i & 63)] = fb;
+            if (role == 0) a.eHAB[soff + i] = make_double2(fa, fb);   // for the x-pass (after the first grid barrier)
         }
     }
     if (tid == 0) mbar_init(mbar);
@@ -302,8 +307,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     // lane block at step t: lane f is in A for t < LA, lane c in B for t < LB
     auto sh_f = [&](int st) { return st < a.LA ? ehA : ehB; };          // slab tables (shared)
     auto sh_c = [&](int st) { return st < a.LB ? ehB : ehA; };
-    auto gl_f = [&](int st) { return st < a.LA ? a.eHA : a.eHB; };      // whole-grid tables (global)
-    auto gl_c = [&](int st) { return st < a.LB ? a.eHB : a.eHA; };
+
     const int zb = r * 64 + t;   // slab index of (y = r, z = t); + 8 j of z
     const int zbe = r * EHP + t; // the same point in the factor tables
 
@@ -339,7 +343,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
         for (int task = gwarp; task < 2 * (P64 / 4); task += nwarps) {
             const bool full = task >= P64 / 4;
             const int c = (full ? task - P64 / 4 : task) * 4 + cq;
-            xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, gl_f(st), gl_c(st), scratch, c, t, tw, tab, rMd);
+            xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, a.eHAB, st >= a.LA, st < a.LB, scratch, c, t, tw, tab,
+                  rMd);
         }
         if (!grid_sync(ctr, a.err, ++bidx)) return;
 
