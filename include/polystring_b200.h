@@ -41,6 +41,7 @@ extern "C" {
 /* MDE schemes, Config::algo_mde_type (src/Config.cc:1099-1111) */
 #define PS_MDE_RQM4 0            /* "RQM4" / "OS4": src/RQM4.cc              */
 #define PS_MDE_OS2 1             /* "OS2" / "PseudoSpectral": src/PseudoSpectral.cc */
+#define PS_MDE_ETDRK4 2          /* "ETDRK4": src/Etdrk4_PBC.cc (Cox-Matthews) */
 /* SCFT field update, Config::algo_scft_type (src/Config.cc:1219-1235) */
 #define PS_SCFT_EM 0
 #define PS_SCFT_ANDERSON 1
@@ -104,9 +105,15 @@ int ps_measure_fp64_peak(double* tflops);
 
 /* RQM4(const UnitCell&, Lx, Ly, Lz, ds)            src/RQM4.cc:9-16
  * PseudoSpectral(const UnitCell&, Lx, Ly, Lz, ds)  src/PseudoSpectral.cc:190-195
- * scheme = PS_MDE_RQM4 or PS_MDE_OS2. */
+ * Etdrk4_PBC(const UnitCell&, Lx, Ly, Lz, ds)      src/Etdrk4_PBC.cc:12-24 (M = 32)
+ * scheme = PS_MDE_RQM4, PS_MDE_OS2 or PS_MDE_ETDRK4.  ETDRK4 uses the
+ * orthogonal k^2 table, as Etdrk4_PBC does. */
 int ps_updater_create(int scheme, const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds,
                       ps_updater** out);
+/* Etdrk4_PBC(const UnitCell&, Lx, Ly, Lz, ds, M)   include/Etdrk4_PBC.h:47-51:
+ * M contour points for the coefficients (M >= 1). */
+int ps_updater_create_etdrk4(const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds, int M,
+                             ps_updater** out);
 /* Updater::clone() (include/Updater.h:67) */
 int ps_updater_clone(const ps_updater* u, ps_updater** out);
 void ps_updater_destroy(ps_updater* u);
@@ -159,6 +166,9 @@ typedef struct ps_model_ab_params {
     int compressible;          /* [Model] is_compressible                       */
     int contour;               /* 0 trapezoid, 1 Simpson (Simpson / Quad4_Closed
                                   by parity of Ms, src/Model_AB.cc:713-735)     */
+    int etdrk4_M;              /* [Algorithm_MDE] etdrk4_M: ETDRK4 contour points;
+                                  <= 0 gives Etdrk4_PBC's default 32
+                                  (src/Model_AB.cc:746-763)                     */
 } ps_model_ab_params;
 
 /* Model_AB::init (src/Model_AB.cc:85-134) for a periodic cell */

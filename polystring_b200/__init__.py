@@ -85,6 +85,19 @@ class PseudoSpectral(_Updater):
     scheme = 1
 
 
+class Etdrk4_PBC(_Updater):
+    """Cox-Matthews ETDRK4 with contour-integral coefficients (src/Etdrk4_PBC.cc),
+    M contour points (include/Etdrk4_PBC.h:47-51, default 32)."""
+    scheme = 2
+
+    def __init__(self, cell, Lx, Ly, Lz, ds, M=32):
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_updater_create_etdrk4(ctypes.byref(cell), Lx, Ly, Lz, ds, M, ctypes.byref(h)))
+        self._h = h
+        self.shape = (Lx, Ly, Lz)
+        self.M = Lx * Ly * Lz
+
+
 def density(rule, q, qc, ds, cc):
     """phi = cc ds sum_s c_s q[s] qc[n-s] (Simpson / Quad4 / trapezoid)."""
     r = RULES[rule] if isinstance(rule, str) else int(rule)
@@ -104,7 +117,7 @@ def grid_mean(x_cuda):
 
 
 def _params(dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft="EM", n_anderson=5,
-            compressible=False, contour="Simpson"):
+            compressible=False, contour="Simpson", etdrk4_M=0):
     """ps_model_ab_params of one Model_AB (the [Model] / [Grid] / [Algorithm_*] values of a config)."""
     Lx, Ly, Lz = shape
     p = capi.ModelABParamsC()
@@ -118,6 +131,7 @@ def _params(dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft=
     p.n_anderson = n_anderson
     p.compressible = 1 if compressible else 0
     p.contour = capi.CONTOUR[contour.upper()]
+    p.etdrk4_M = etdrk4_M
     return p
 
 
@@ -126,9 +140,9 @@ class ModelAB:
     CUDA graph (propagators, Q, densities, field update)."""
 
     def __init__(self, dim, shape, cell, Ms, chiN, lam=(0.05, 0.05, 5.0), mde="RQM4", scft="EM",
-                 n_anderson=5, compressible=False, contour="Simpson"):
+                 n_anderson=5, compressible=False, contour="Simpson", etdrk4_M=0):
         Lx, Ly, Lz = shape
-        p = _params(dim, shape, cell, Ms, chiN, lam, mde, scft, n_anderson, compressible, contour)
+        p = _params(dim, shape, cell, Ms, chiN, lam, mde, scft, n_anderson, compressible, contour, etdrk4_M)
         h = ctypes.c_void_p()
         capi.check(lib().ps_model_ab_create(ctypes.byref(p), ctypes.byref(h)))
         self._h = h

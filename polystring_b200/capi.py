@@ -20,7 +20,7 @@ PS_ERR_STATE = -6
 # contour points the fixed table of ps_density_solve_device_noalloc holds
 PS_DENSITY_NOALLOC_MAX_LEN = 8192
 
-MDE = {"RQM4": 0, "OS4": 0, "OS2": 1, "PSEUDOSPECTRAL": 1}
+MDE = {"RQM4": 0, "OS4": 0, "OS2": 1, "PSEUDOSPECTRAL": 1, "ETDRK4": 2}
 SCFT = {"EM": 0, "ANDERSON": 1}
 CONTOUR = {"TRAPEZOID": 0, "TRAPEZOIDAL": 0, "SIMPSON": 1}
 RULES = {"trapezoid": 0, "simpson": 1, "quad4_closed": 2, "quad4_open": 3,
@@ -46,7 +46,8 @@ class ModelABParamsC(ctypes.Structure):
                 ("cell", UnitCellC), ("sA", ctypes.c_int), ("sB", ctypes.c_int),
                 ("chiN", ctypes.c_double), ("lamA", ctypes.c_double), ("lamB", ctypes.c_double),
                 ("lamYita", ctypes.c_double), ("mde", ctypes.c_int), ("scft", ctypes.c_int),
-                ("n_anderson", ctypes.c_int), ("compressible", ctypes.c_int), ("contour", ctypes.c_int)]
+                ("n_anderson", ctypes.c_int), ("compressible", ctypes.c_int), ("contour", ctypes.c_int),
+                ("etdrk4_M", ctypes.c_int)]
 
 
 SIGNATURES = [
@@ -56,6 +57,8 @@ SIGNATURES = [
     ("ps_measure_fp64_peak", ctypes.c_int, [_dp]),
     ("ps_updater_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(UnitCellC), ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)]),
+    ("ps_updater_create_etdrk4", ctypes.c_int, [ctypes.POINTER(UnitCellC), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ps_updater_clone", ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     ("ps_updater_destroy", None, [_vp]),
     ("ps_updater_solve", ctypes.c_int, [_vp, _dp, _dp, ctypes.c_int]),

@@ -55,7 +55,7 @@ void tuning_note(const char* line) {
 }
 
 void PairChain::autotune(cudaStream_t st) {
-    if (plan_.naxes < 2 || !tuning_enabled()) return;
+    if (plan_.naxes < 2 || scheme_ == SCHEME_ETDRK4 || !tuning_enabled()) return;
     const TuneKey key{Lx_, Ly_, Lz_, scheme_, nbatch_, batched_tables_ ? 1 : 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);

@@ -68,10 +68,22 @@ const char* ps_last_error(void) { return g_last_error.c_str(); }
 int ps_updater_create(int scheme, const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds, ps_updater** out) {
     return guarded([&] {
         if (!out) throw Error(PS_ERR_INVALID, "null output handle");
-        if (scheme != PS_MDE_RQM4 && scheme != PS_MDE_OS2) throw Error(PS_ERR_INVALID, "unknown MDE scheme");
+        if (scheme != PS_MDE_RQM4 && scheme != PS_MDE_OS2 && scheme != PS_MDE_ETDRK4)
+            throw Error(PS_ERR_INVALID, "unknown MDE scheme");
         Cell c = to_cell(cell);
         check_dims(c.dim, Lx, Ly, Lz);
-        *out = new ps_updater{new UpdaterCtx(scheme == PS_MDE_RQM4 ? SCHEME_RQM4 : SCHEME_OS2, c, Lx, Ly, Lz, ds)};
+        const int sc = scheme == PS_MDE_RQM4 ? SCHEME_RQM4 : scheme == PS_MDE_OS2 ? SCHEME_OS2 : SCHEME_ETDRK4;
+        *out = new ps_updater{new UpdaterCtx(sc, c, Lx, Ly, Lz, ds)};
+    });
+}
+
+int ps_updater_create_etdrk4(const ps_unit_cell* cell, int Lx, int Ly, int Lz, double ds, int M, ps_updater** out) {
+    return guarded([&] {
+        if (!out) throw Error(PS_ERR_INVALID, "null output handle");
+        if (M < 1) throw Error(PS_ERR_INVALID, "ETDRK4 needs at least one contour point");
+        Cell c = to_cell(cell);
+        check_dims(c.dim, Lx, Ly, Lz);
+        *out = new ps_updater{new UpdaterCtx(SCHEME_ETDRK4, c, Lx, Ly, Lz, ds, M)};
     });
 }
 
@@ -148,7 +160,8 @@ static ModelABParams to_params(const ps_model_ab_params* p) {
     if (!p) throw Error(PS_ERR_INVALID, "null parameters");
     check_dims(p->dim, p->Lx, p->Ly, p->Lz);
     if (p->cell.dim != p->dim) throw Error(PS_ERR_INVALID, "cell dimension differs from grid dimension");
-    if (p->mde != PS_MDE_RQM4 && p->mde != PS_MDE_OS2) throw Error(PS_ERR_INVALID, "unknown MDE scheme");
+    if (p->mde != PS_MDE_RQM4 && p->mde != PS_MDE_OS2 && p->mde != PS_MDE_ETDRK4)
+        throw Error(PS_ERR_INVALID, "unknown MDE scheme");
     if (p->scft != PS_SCFT_EM && p->scft != PS_SCFT_ANDERSON) throw Error(PS_ERR_INVALID, "unknown SCFT algorithm");
     ModelABParams q;
     q.dim = p->dim; q.Lx = p->Lx; q.Ly = p->Ly; q.Lz = p->Lz;
@@ -157,6 +170,7 @@ static ModelABParams to_params(const ps_model_ab_params* p) {
     q.lamA = p->lamA; q.lamB = p->lamB; q.lamYita = p->lamYita;
     q.mde = p->mde; q.scft = p->scft; q.n_anderson = p->n_anderson;
     q.compressible = p->compressible; q.contour = p->contour;
+    q.etd_M = p->etdrk4_M;
     return q;
 }
 

@@ -203,7 +203,14 @@ PairChain::PairChain(int Lx, int Ly, int Lz, int scheme, int nbatch)
     }
     // attributes and twiddles before any capture
     const LineGeom& in = plan_.ax[0];
-    if (plan_.naxes == 1) {
+    if (scheme == SCHEME_ETDRK4) {
+        if (nbatch != 1) throw Error(-2, "ETDRK4 chains are not batched");
+        etd_.alloc(10 * (size_t)M_);
+        for (int a = 0; a < plan_.naxes; a++) {
+            prepare_line_pass(MODE_FWD, plan_.ax[a]);
+            prepare_line_pass(MODE_INV, plan_.ax[a]);
+        }
+    } else if (plan_.naxes == 1) {
         prepare_line_pass(scheme == SCHEME_RQM4 ? MODE_FULL_RQM4 : MODE_FULL_OS2, in);
     } else {
         const LineGeom& out = plan_.ax[plan_.naxes - 1];
@@ -244,6 +251,8 @@ void PairChain::set_tables_batched(const std::vector<double>& L1, const std::vec
 }
 
 int PairChain::launches_per_step() const {
+    // slices, 4 x (forward transform, combine, inverse transform), 3 nonlinear terms, store
+    if (scheme_ == SCHEME_ETDRK4) return 1 + 4 * (2 * plan_.naxes + 1) + 3 + 1;
     if (plan_.naxes == 1) return 1;
     if (scheme_ == SCHEME_RQM4) return plan_.naxes == 3 ? 8 : 4;
     return plan_.naxes == 3 ? 4 : 2;
@@ -267,6 +276,11 @@ void PairChain::enqueue(double* hf, double* hc, long hist_bstride, int nsteps, c
     const LineGeom& out = plan_.ax[na - 1];
     const LineGeom* mid = (na == 3) ? &plan_.ax[1] : nullptr;
     const bool rq = (scheme_ == SCHEME_RQM4);
+    if (scheme_ == SCHEME_ETDRK4) {
+        if (hist_bstride != 0 || fac_bstride != 0) throw Error(-2, "ETDRK4 chains are not batched");
+        enqueue_etd(hf, hc, nsteps, lf, lc, st, c_in_fixed, c_out_fixed);
+        return;
+    }
 
     for (int t = 0; t < nsteps; t++) {
         StepPtrs p = base;
@@ -390,11 +404,14 @@ ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
         throw Error(-4, "contour quadrature precondition fails for Ms = [" + std::to_string(p.sA) + ", " +
                             std::to_string(p.sB) + "]");
     PS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
-    chain_ = new PairChain(p.Lx, p.Ly, p.Lz, p.mde == 1 ? SCHEME_OS2 : SCHEME_RQM4, 1);
+    chain_ = new PairChain(p.Lx, p.Ly, p.Lz, p.mde == 1 ? SCHEME_OS2 : p.mde == 2 ? SCHEME_ETDRK4 : SCHEME_RQM4, 1);
     // k tables.  ds of the two blocks agree to within two ulps (both round
     // 1/(LA+LB)); the packed lanes share the block-A table.
     if (p.mde == 1) {
         chain_->set_tables(k_laplacian(p_.cell, p.Lx, p.Ly, p.Lz, dsA_), {});
+    } else if (p.mde == 2) {
+        // Etdrk4_PBC(uc, Lx, Ly, Lz, dsA, etdrk4_M) (Model_AB.cc:746-763; M = 32 when unset)
+        chain_->set_tables_etd(k2_orthogonal(p_.cell, p.Lx, p.Ly, p.Lz), dsA_, p.etd_M > 0 ? p.etd_M : 32);
     } else {
         std::vector<double> k2 = k2_orthogonal(p_.cell, p.Lx, p.Ly, p.Lz);
         std::vector<double> L1(M_), L2(M_);
@@ -628,6 +645,13 @@ void ModelAB::enqueue_propagate(cudaStream_t s) {
         sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, s, sweep_variant_);
         return;
     }
+    if (p_.mde == 2) {
+        // ETDRK4 takes the fields themselves: N(q) = -w q
+        LaneFactors lf{{wA_.p, wB_.p}, {wA_.p, wB_.p}, LA_};
+        LaneFactors lc{{wB_.p, wA_.p}, {wB_.p, wA_.p}, LB_};
+        chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, s);
+        return;
+    }
     LaneFactors lf{{eFA_.p, eFB_.p}, {eHA_.p, eHB_.p}, LA_};
     LaneFactors lc{{eFB_.p, eFA_.p}, {eHB_.p, eHA_.p}, LB_};
     chain_->enqueue(hf_.p, hc_.p, 0, Ns_, lf, lc, 0, s);
@@ -824,8 +848,8 @@ void ModelAB::get(int which, double* out, bool device_dst) {
 // ---------------------------------------------------------------------------
 // UpdaterCtx
 // ---------------------------------------------------------------------------
-UpdaterCtx::UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, double ds)
-    : scheme_(scheme), Lx_(Lx), Ly_(Ly), Lz_(Lz), cell_(cell), ds_(ds) {
+UpdaterCtx::UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, double ds, int etd_M)
+    : scheme_(scheme), Lx_(Lx), Ly_(Ly), Lz_(Lz), cell_(cell), ds_(ds), etd_M_(etd_M) {
     if (!(ds > 0)) throw Error(-1, "ds must be positive");
     cell_init(cell_);
     M_ = (long)Lx * Ly * Lz;
@@ -833,6 +857,8 @@ UpdaterCtx::UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, dou
     chain_ = new PairChain(Lx, Ly, Lz, scheme, 1);
     if (scheme == SCHEME_OS2) {
         chain_->set_tables(k_laplacian(cell_, Lx, Ly, Lz, ds), {});
+    } else if (scheme == SCHEME_ETDRK4) {
+        chain_->set_tables_etd(k2_orthogonal(cell_, Lx, Ly, Lz), ds, etd_M);
     } else {
         std::vector<double> k2 = k2_orthogonal(cell_, Lx, Ly, Lz);
         std::vector<double> L1(M_), L2(M_);
@@ -855,12 +881,19 @@ UpdaterCtx::~UpdaterCtx() {
     if (st_) cudaStreamDestroy(st_);
 }
 
-UpdaterCtx* UpdaterCtx::clone() const { return new UpdaterCtx(scheme_, cell_, Lx_, Ly_, Lz_, ds_); }
+UpdaterCtx* UpdaterCtx::clone() const { return new UpdaterCtx(scheme_, cell_, Lx_, Ly_, Lz_, ds_, etd_M_); }
 
 void UpdaterCtx::solve_device(const double* w, double* qs, int len, cudaStream_t st) {
     if (len < 1) throw Error(-1, "propagator length must be at least 1");
     if (len == 1) return;
     if (!st) st = st_;
+    if (scheme_ == SCHEME_ETDRK4) {
+        // Etdrk4_PBC::solve (Etdrk4_PBC.cc:110-184) reads w itself
+        LaneFactors lf{{w, w}, {w, w}, len};
+        LaneFactors lc{{zero_.p, zero_.p}, {zero_.p, zero_.p}, len};
+        chain_->enqueue(qs, nullptr, 0, len - 1, lf, lc, 0, st, zero_.p, scratch_.p);
+        return;
+    }
     // exp(-w ds/2), exp(-w ds/4) (RQM4.cc:49-52, PseudoSpectral.cc:234-235)
     launch_factors(w, w, M_, ds_, ds_, eF_.p, eH_.p, eF_.p + M_, eH_.p + M_, 1, 0, st);
     // lane c carries nothing: zero factors, zero input, scratch output

@@ -51,7 +51,7 @@ void set_tile_elems(LineGeom& g, int elems);
 const char* tuning_log();
 void tuning_note(const char* line);   // appends one line to the tuning log
 
-enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1 };
+enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1, SCHEME_ETDRK4 = 2 };
 
 // Which Boltzmann factors a lane uses at step t: set 0 before switch_t,
 // set 1 from switch_t on (a chain crossing the A/B junction).
@@ -100,8 +100,12 @@ public:
     void set_tables(const std::vector<double>& L1, const std::vector<double>& L2);
     // batched tables: nbatch consecutive tables of M values each
     void set_tables_batched(const std::vector<double>& L1, const std::vector<double>& L2);
+    // ETDRK4 (etdrk4.cu): E, E2, Q, f1, f2, f3 from the k2_orthogonal table,
+    // Mc contour points (Etdrk4_PBC.cc:43-99)
+    void set_tables_etd(const std::vector<double>& k2, double ds, int Mc);
     // c_in_fixed / c_out_fixed: lane c reads and writes fixed slices instead
-    // of a history (single-chain solves)
+    // of a history (single-chain solves).  ETDRK4: the factor slots of lf and
+    // lc carry the fields w of each lane's blocks.
     void enqueue(double* hf, double* hc, long hist_bstride, int nsteps, const LaneFactors& lf,
                  const LaneFactors& lc, long fac_bstride, cudaStream_t st, const double* c_in_fixed = nullptr,
                  double* c_out_fixed = nullptr);
@@ -121,10 +125,15 @@ public:
     const double* L2() const { return L2_.p; }
 
 private:
+    void enqueue_etd(double* hf, double* hc, int nsteps, const LaneFactors& lf, const LaneFactors& lc,
+                     cudaStream_t st, const double* c_in_fixed, double* c_out_fixed);
+    void transform(double2* z, int mode, cudaStream_t st) const;
+
     int Lx_, Ly_, Lz_, scheme_, nbatch_;
     long M_;
     AxisPlan plan_;
     DevBuf z_[3], u_[2], L1_, L2_, half_;
+    DevBuf etd_, etdtab_;   // ETDRK4: V, Nv, A, Na, Nb (packed spectra); E, E2, Q, f1, f2, f3
     bool batched_tables_ = false;
 };
 
@@ -135,6 +144,7 @@ struct ModelABParams {
     int sA, sB;
     double chiN, lamA, lamB, lamYita;
     int mde, scft, n_anderson, compressible, contour;
+    int etd_M;   // ETDRK4 contour points (Etdrk4_PBC's M)
 };
 
 class ModelAB {
@@ -236,10 +246,10 @@ private:
     int launches_per_prop_ = 0;
 };
 
-// Single propagator updater behind the Updater C-ABI (RQM4 / OS2)
+// Single propagator updater behind the Updater C-ABI (RQM4 / OS2 / ETDRK4)
 class UpdaterCtx {
 public:
-    UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, double ds);
+    UpdaterCtx(int scheme, const Cell& cell, int Lx, int Ly, int Lz, double ds, int etd_M = 32);
     ~UpdaterCtx();
     UpdaterCtx* clone() const;
     void solve_device(const double* w, double* qs, int len, cudaStream_t st);
@@ -250,6 +260,7 @@ private:
     int scheme_, Lx_, Ly_, Lz_;
     Cell cell_;
     double ds_;
+    int etd_M_;
     long M_;
     PairChain* chain_ = nullptr;
     DevBuf eF_, eH_, zero_, scratch_, dw_, dqs_;

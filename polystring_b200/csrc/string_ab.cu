@@ -190,6 +190,7 @@ StringAB::StringAB(const ModelABParams& p, int m, int max_iter, int lo, int hi)
     std::vector<double> cA, cB;
     if (!contour_weights(ruleA, LA_, cA) || !contour_weights(ruleB, LB_, cB))
         throw Error(-4, "contour quadrature precondition fails");
+    if (p.mde != 0 && p.mde != 1) throw Error(-2, "string images use RQM4 or OS2");
     PS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     chain_ = new PairChain(p.Lx, p.Ly, p.Lz, p.mde == 1 ? SCHEME_OS2 : SCHEME_RQM4, nloc_);
     if (p.mde == 1) {

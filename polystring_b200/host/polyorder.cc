@@ -369,8 +369,6 @@ void Density::update(const Propagator& q, const Propagator& qc, double cc) {
 // Model_AB
 // ---------------------------------------------------------------------------
 Model_AB::Model_AB(const Config& cfg) : Lx_(cfg.Lx()), Ly_(cfg.Ly()), Lz_(cfg.Lz()) {
-    if (cfg.algo_mde_type() == AlgorithmMDEType::ETDRK4)
-        throw std::runtime_error("MDE algorithm ETDRK4 is not provided by the B200 backend (RQM4, OS2)");
     std::string confine = upper(cfg.get_string("Grid", "confine_geometry", "NONE"));
     if (!(confine == "NONE" || confine.empty()))
         throw std::runtime_error("only periodic cells (confine_geometry = None) are provided by the B200 backend");
@@ -387,7 +385,13 @@ Model_AB::Model_AB(const Config& cfg) : Lx_(cfg.Lx()), Ly_(cfg.Ly()), Lz_(cfg.Lz
     std::vector<double> lam = cfg.lam();
     if (lam.size() < 3) throw std::runtime_error("[Algorithm_SCFT] lam needs three entries");
     p.lamA = lam[0]; p.lamB = lam[1]; p.lamYita = lam[2];
-    p.mde = cfg.algo_mde_type() == AlgorithmMDEType::OS2 ? PS_MDE_OS2 : PS_MDE_RQM4;
+    // Model_AB::init_propagator (Model_AB.cc:740-790): ETDRK4 is Etdrk4_PBC (Cox-Matthews)
+    switch (cfg.algo_mde_type()) {
+    case AlgorithmMDEType::OS2: p.mde = PS_MDE_OS2; break;
+    case AlgorithmMDEType::ETDRK4: p.mde = PS_MDE_ETDRK4; break;
+    default: p.mde = PS_MDE_RQM4; break;
+    }
+    p.etdrk4_M = cfg.etdrk4_M();
     p.scft = cfg.algo_scft_type() == AlgorithmSCFTType::ANDERSON ? PS_SCFT_ANDERSON : PS_SCFT_EM;
     p.n_anderson = cfg.n_Anderson_mixing();
     p.compressible = cfg.is_compressible() ? 1 : 0;

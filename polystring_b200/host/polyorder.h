@@ -67,6 +67,8 @@ public:
     std::vector<double> lam() const { return get_list("Algorithm_SCFT", "lam"); }
     bool is_compressible() const { return get_bool("Model", "is_compressible"); }
     int n_Anderson_mixing() const { return get_integer("Algorithm_SCFT", "n_Anderson_mixing", 5); }
+    // Config::etdrk4_M (Config.cc:1203-1205); empty or <= 0: Etdrk4_PBC's default
+    int etdrk4_M() const { return get_integer("Algorithm_MDE", "etdrk4_M", 0); }
     int min_iter() const { return get_integer("Algorithm_SCFT", "min_iter", 1); }
     int max_iter() const { return get_integer("Algorithm_SCFT", "max_iter", 1); }
     double thresh_residual() const { return get_double("Algorithm_SCFT", "thresh_residual", 0.0); }

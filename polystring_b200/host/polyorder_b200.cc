@@ -19,9 +19,9 @@ static void print_params(const polyorder::Config& cfg) {
     std::printf("cell system %d a %.17g b %.17g c %.17g\n", c.system, c.a, c.b, c.c);
     std::printf("Ms %d %d chiN %.17g\n", (int)Ms.at(0), (int)Ms.at(1), cfg.chiN());
     std::printf("lam %.17g %.17g %.17g\n", lam.at(0), lam.at(1), lam.at(2));
-    std::printf("mde %d scft %d contour %d cellopt %d init %d\n", (int)cfg.algo_mde_type(), (int)cfg.algo_scft_type(),
-                (int)cfg.algo_contour_integration_type(), (int)cfg.algo_cell_optimization_type(),
-                (int)cfg.get_grid_init_type());
+    std::printf("mde %d scft %d contour %d cellopt %d init %d etdrk4_M %d\n", (int)cfg.algo_mde_type(),
+                (int)cfg.algo_scft_type(), (int)cfg.algo_contour_integration_type(),
+                (int)cfg.algo_cell_optimization_type(), (int)cfg.get_grid_init_type(), cfg.etdrk4_M());
     std::printf("n_anderson %d compressible %d max_iter %d min_iter %d record %d thresh %.17g\n",
                 cfg.n_Anderson_mixing(), (int)cfg.is_compressible(), cfg.max_iter(), cfg.min_iter(),
                 cfg.record_interval(), cfg.thresh_residual());

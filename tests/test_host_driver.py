@@ -120,3 +120,17 @@ def test_string_driver_without_gpu_fails_cleanly(tmp_path):
     r = subprocess.run([build.STRING_EXE, str(tmp_path / "paramString.ini")], capture_output=True, text=True)
     assert r.returncode == 1 and "error" in r.stderr
     assert "Initializing string by two ends" in r.stdout
+
+
+@pytest.mark.parametrize("m_value,expect", [("", "0"), ("16", "16")])
+def test_check_reads_etdrk4_keys(exe, tmp_path, golden, m_value, expect):
+    """algorithm = ETDRK4 in [Algorithm_MDE] selects Etdrk4_PBC (enum value 2:
+    OS2, RQM4, ETDRK4) and etdrk4_M is passed through (empty: the default)."""
+    d, _, _ = _case(tmp_path, golden, "1d")
+    text = (d / "param.ini").read_text()
+    text = text.replace("algorithm = OS2", "algorithm = ETDRK4", 1).replace("etdrk4_M =", "etdrk4_M = " + m_value, 1)
+    (d / "param.ini").write_text(text)
+    r = subprocess.run([exe, "--check", str(d / "param.ini")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    v = _parse(r.stdout)
+    assert v["mde"][0] == "2" and v["mde"][10] == expect
