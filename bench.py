@@ -225,7 +225,9 @@ def cpu_batch_baseline(seconds, threads, n=256):
     sample (seconds split between them), applied to every solve's 2 Ns M
     steps, as one host process running the solves one after another would."""
     from polystring_b200 import workloads
-    specs = workloads.uneven_solves(n)
+    n_ab, n_abc = c5_split(n)
+    specs = workloads.uneven_solves(n_ab)
+    tri = workloads.uneven_triblocks(n_abc)
     rates, samples = {}, []
     shapes = sorted({tuple(sp["shape"]) for sp in specs})
     for shp in shapes:
@@ -234,7 +236,8 @@ def cpu_batch_baseline(seconds, threads, n=256):
         r, nsteps, dt = cpu_propagation_rate(3, shp, (L, L, L), sp["Ms"], sp["wA"], seconds / len(shapes), threads)
         rates[shp] = r
         samples.append("%d steps at %d^3 in %.1f s" % (nsteps, shp[0], dt))
-    work = [2 * (sp["Ms"][0] + sp["Ms"][1] - 2) * int(np.prod(sp["shape"])) for sp in specs]
+    specs = specs + tri
+    work = [2 * (sum(sp["Ms"]) - len(sp["Ms"])) * int(np.prod(sp["shape"])) for sp in specs]
     t = sum(w / rates[tuple(sp["shape"])] for w, sp in zip(work, specs))
     return {"gridpt_steps_per_s": sum(work) / t, "cores": threads, "kind": "port",
             "sample": "oracle RQM4 propagators, %d OpenMP threads: %s; propagation only"
@@ -285,40 +288,65 @@ def string_method(ps, fp64=(37.0, "nominal"), iters=10):
             "timing": "host wall clock around synchronised replays"}
 
 
+def c5_split(n):
+    """C5's n solves: three quarters AB diblocks, one quarter ABC triblocks."""
+    return n - n // 4, n // 4
+
+
 def uneven_batch(ps, n=256, iters=2):
     """Secondary result: the C5 workload -- n = 256 independent solves of
-    uneven grids (32^3, 48^3, 64^3) and Ns (64, 128, 256) -- advanced as one
-    batch for `iters` Anderson iterations (of the 300 the workload runs),
-    against the same solves run one after another, each on its own fastest
-    single path (persistent sweeps on these cubic grids).  Device time by
-    CUDA events."""
+    uneven grids (32^3, 48^3, 64^3) and Ns (64, 128, 256), 192 AB diblocks
+    and 64 linear ABC triblocks -- advanced as one batch for `iters` Anderson
+    iterations (of the 300 the workload runs), against the same solves run
+    one after another, each on its own fastest single path (persistent sweeps
+    for the AB solves on these cubic grids, line passes for the triblocks).
+    Device time by CUDA events."""
     from polystring_b200 import workloads
-    specs = workloads.uneven_solves(n)
+    n_ab, n_abc = c5_split(n)
+    specs = workloads.uneven_solves(n_ab)
+    tri = workloads.uneven_triblocks(n_abc)
 
     def model_args(sp):
         return dict(dim=sp["dim"], shape=sp["shape"], cell=ps.make_cell(3, "CUBIC", sp["cell"][1][0]), Ms=sp["Ms"],
                     chiN=sp["chiN"], lam=sp["lam"], scft=sp["scft"], n_anderson=sp["n_anderson"])
-    b = ps.BatchAB([model_args(sp) for sp in specs])
+
+    def abc_args(sp):
+        return dict(dim=sp["dim"], shape=sp["shape"], cell=ps.make_cell(3, "CUBIC", sp["cell"][1][0]), Ms=sp["Ms"],
+                    chi=sp["chi"], lam=sp["lam"], scft=sp["scft"], n_anderson=sp["n_anderson"])
+    b = ps.BatchAB([model_args(sp) for sp in specs], [abc_args(sp) for sp in tri])
     for k, sp in enumerate(specs):
         b.set_fields(k, sp["wA"], sp["wB"])
+    for j, sp in enumerate(tri):
+        b.set_fields(n_ab + j, *sp["w"])
     b.update(1)
     tb = b.update_timed(iters) / 1e3
     work = b.gridpoint_steps() * iters
     launches = b.launches_per_iteration()
     del b
-    ts = 0.0
+    ts = ts_abc = 0.0
     for sp in specs:
         m = ps.ModelAB(**model_args(sp))
         m.set_fields(sp["wA"], sp["wB"])
         m.update(1)
         ts += m.update_timed(iters)[0] / 1e3
         del m
+    for sp in tri:
+        m = ps.ModelABC(**abc_args(sp)).set_fields(*sp["w"])
+        m.update(1)
+        m.synchronize()
+        t0 = time.perf_counter()
+        m.update(iters)
+        m.synchronize()
+        ts_abc += time.perf_counter() - t0
+        del m
     sizes = sorted({sp["shape"][0] for sp in specs})
-    return {"config": "C5: %d solves, grids %s^3, Ns 64/128/256, Anderson(10), %d of 300 iterations timed"
-                      % (n, sizes, iters),
-            "batch_gridpt_steps_per_s": work / tb, "sequential_gridpt_steps_per_s": work / ts,
-            "speedup_vs_sequential": ts / tb, "launches_per_batch_iteration": launches,
-            "timing": "CUDA events on the batch stream / each solve's stream"}
+    return {"config": "C5: %d solves (%d AB, %d linear ABC), grids %s^3, Ns 64/128/256, Anderson(10), "
+                      "%d of 300 iterations timed" % (n, n_ab, n_abc, sizes, iters),
+            "batch_gridpt_steps_per_s": work / tb, "sequential_gridpt_steps_per_s": work / (ts + ts_abc),
+            "speedup_vs_sequential": (ts + ts_abc) / tb, "launches_per_batch_iteration": launches,
+            "sequential_s": {"ab": ts, "abc": ts_abc},
+            "timing": "CUDA events on the batch stream and each AB solve's stream; host clock around "
+                      "synchronised runs for each ABC solve"}
 
 
 def adjoint_c4(ps, thresh=1e-9, max_iter=2000):

@@ -228,6 +228,42 @@ int ps_model_ab_launches_per_propagate(ps_model_ab* m);
 /* CUDA stream of the context (cudaStream_t as void*) */
 void* ps_model_ab_stream(ps_model_ab* m);
 
+/* ---- Model_ABC: a linear A-B-C triblock melt (no counterpart in the
+ * reference, which has no periodic ABC melt model) -------------------------
+ * Model_AB's steps with a third block and field: blocks of sA, sB, sC
+ * contour points (ds = 1 / (sA + sB + sC - 3) up to rounding), Simpson or
+ * Quad4_Closed by parity of each block's Ms, targets
+ *   wA* = chiAB phiB + chiAC phiC + eta, wB* = chiAB phiA + chiBC phiC + eta,
+ *   wC* = chiAC phiA + chiBC phiB + eta,
+ * simple mixing with eta += lamYita (phiA + phiB + phiC - 1), or Anderson
+ * mixing (one ring per field, one coefficient set) with
+ *   eta = (wA + wB + wC - chiAB (phiA + phiB) - chiBC (phiB + phiC)
+ *          - chiAC (phiA + phiC)) / 3;
+ * H = mean(chiAB phiA phiB + chiBC phiB phiC + chiAC phiA phiC
+ *          - wA phiA - wB phiB - wC phiC) - ln Q.
+ * Incompressible, RQM4, orthogonal cells. */
+typedef struct ps_model_abc_params {
+    int dim, Lx, Ly, Lz;
+    ps_unit_cell cell;
+    int sA, sB, sC;
+    double chiAB, chiBC, chiAC;            /* times N                         */
+    double lamA, lamB, lamC, lamYita;
+    int scft;                              /* PS_SCFT_*                       */
+    int n_anderson;                        /* 1..31                           */
+    int contour;                           /* 0 trapezoid, 1 Simpson / Quad4  */
+} ps_model_abc_params;
+typedef struct ps_model_abc ps_model_abc;
+int ps_model_abc_create(const ps_model_abc_params* p, ps_model_abc** out);
+void ps_model_abc_destroy(ps_model_abc* m);
+int ps_model_abc_set_fields(ps_model_abc* m, const double* wA, const double* wB, const double* wC);
+int ps_model_abc_update(ps_model_abc* m, int n_iter);
+int ps_model_abc_Q(ps_model_abc* m, double* Q);
+int ps_model_abc_H(ps_model_abc* m, double* H, double* Hw, double* Hs);
+int ps_model_abc_residual(ps_model_abc* m, double* res);
+/* which: 0..2 wA, wB, wC; 3..5 phiA, phiB, phiC; 6 eta (M values, host) */
+int ps_model_abc_get(ps_model_abc* m, int which, double* out);
+int ps_model_abc_synchronize(ps_model_abc* m);
+
 /* ---- string method: all images of the string on the device ----------- */
 typedef struct ps_string_ab ps_string_ab;
 /* polystring_AB (scft/polystring_AB.cc:111-152) with m images of the model
@@ -287,6 +323,14 @@ void* ps_string_ab_stream(ps_string_ab* s);
  * the per-pass path. */
 typedef struct ps_batch_ab ps_batch_ab;
 int ps_batch_ab_create(const ps_model_ab_params* p, int n, ps_batch_ab** out);
+/* A batch of n Model_AB solves (members 0 .. n-1) and nq linear ABC
+ * triblock solves (members n .. n+nq-1, see ps_model_abc_params; 2D or 3D
+ * grids; always on grouped line passes).  ps_batch_ab_H / _residual / _get
+ * take either kind of member (_get with the ps_model_abc_get numbering for
+ * ABC members). */
+int ps_batch_ab_create_mixed(const ps_model_ab_params* p, int n, const ps_model_abc_params* q, int nq,
+                             ps_batch_ab** out);
+int ps_batch_ab_set_fields_abc(ps_batch_ab* b, int k, const double* wA, const double* wB, const double* wC);
 void ps_batch_ab_destroy(ps_batch_ab* b);
 int ps_batch_ab_set_fields(ps_batch_ab* b, int k, const double* wA, const double* wB);
 int ps_batch_ab_update(ps_batch_ab* b, int n_iter);

@@ -84,6 +84,16 @@ def lib():
         L.orc_model_ab_Q.restype = ctypes.c_double
         L.orc_model_ab_last_rc.argtypes = [vp]
         L.orc_model_ab_get.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_model_abc_create.argtypes = [ctypes.POINTER(_ABCParams), dp, dp, dp]
+        L.orc_model_abc_create.restype = vp
+        L.orc_model_abc_destroy.argtypes = [vp]
+        L.orc_model_abc_update.argtypes = [vp]
+        L.orc_model_abc_H.argtypes = [vp, dp, dp, dp]
+        L.orc_model_abc_residual.argtypes = [vp]
+        L.orc_model_abc_residual.restype = ctypes.c_double
+        L.orc_model_abc_Q.argtypes = [vp]
+        L.orc_model_abc_Q.restype = ctypes.c_double
+        L.orc_model_abc_get.argtypes = [vp, ctypes.c_int, dp]
         L.orc_string_arclength.argtypes = [dp, ctypes.c_int, ctypes.c_size_t, dp]
         L.orc_string_redistribute.argtypes = [dp, dp, ctypes.c_int, ctypes.c_size_t, dp, dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
@@ -287,6 +297,68 @@ class ModelAB:
     def __del__(self):
         if getattr(self, "h", None):
             lib().orc_model_ab_destroy(self.h)
+            self.h = None
+
+
+class _ABCParams(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int), ("Lx", ctypes.c_int), ("Ly", ctypes.c_int), ("Lz", ctypes.c_int),
+        ("s", ctypes.c_int * 3), ("chi", ctypes.c_double * 3), ("lam", ctypes.c_double * 4),
+        ("scft", ctypes.c_int), ("n_anderson", ctypes.c_int), ("contour", ctypes.c_int),
+        ("k2", ctypes.POINTER(ctypes.c_double))]
+
+
+class ModelABC:
+    """Linear A-B-C triblock melt (defined in scft_oracle.c's Model_ABC block:
+    Model_AB's steps with a third block and field; incompressible, RQM4).
+    chi = (chiAB N, chiBC N, chiAC N); lam = (lamA, lamB, lamC, lamYita)."""
+
+    def __init__(self, dim, shape, lengths, Ms, chi, lam=(0.05, 0.05, 0.05, 5.0), scft="EM", n_anderson=5,
+                 contour="Simpson"):
+        self.shape = tuple(shape)
+        self.M = int(np.prod(shape))
+        self.Ms = tuple(Ms)
+        self._k2 = k2_orthogonal(dim, lengths, shape)
+        self.params = _ABCParams(dim, shape[0], shape[1], shape[2], (ctypes.c_int * 3)(*Ms),
+                                 (ctypes.c_double * 3)(*chi), (ctypes.c_double * 4)(*lam),
+                                 ANDERSON if scft == "Anderson" else EM, n_anderson,
+                                 1 if contour == "Simpson" else 0, _p(self._k2))
+        self.h = None
+
+    def init_fields(self, wA, wB, wC):
+        if self.h:
+            lib().orc_model_abc_destroy(self.h)
+        self._w = [_f64(wA), _f64(wB), _f64(wC)]
+        self.h = lib().orc_model_abc_create(ctypes.byref(self.params), *[_p(w) for w in self._w])
+        return self
+
+    def update(self, n=1):
+        rc = 0
+        for _ in range(n):
+            rc |= lib().orc_model_abc_update(self.h)
+        return rc
+
+    def H(self):
+        H, Hw, Hs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        lib().orc_model_abc_H(self.h, ctypes.byref(H), ctypes.byref(Hw), ctypes.byref(Hs))
+        return H.value, Hw.value, Hs.value
+
+    def residual(self):
+        return lib().orc_model_abc_residual(self.h)
+
+    def Q(self):
+        return lib().orc_model_abc_Q(self.h)
+
+    def get(self, name):
+        idx = {"wA": 0, "wB": 1, "wC": 2, "phiA": 3, "phiB": 4, "phiC": 5, "yita": 6}[name]
+        out = np.zeros(self.shape)
+        if lib().orc_model_abc_get(self.h, idx, _p(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_model_abc_destroy(self.h)
             self.h = None
 
 

@@ -24,6 +24,8 @@
  *                   :713-735 (quadrature choice)
  *   Field / Yita    src/Field.cc:51-59, src/Yita.cc:49-55
  *   FieldAX         src/FieldAX.cc:152-427 (ring history, B, U, V, W, D)
+ *   Model_ABC       (no reference counterpart) linear ABC triblock melt built
+ *                   from the Model_AB steps above, defined in its own block
  *   string method   scft/polystring_AB.cc:283-329 (arc length, per-point
  *                   natural cubic spline, ends restored)
  *
@@ -1024,6 +1026,217 @@ int orc_model_ab_get(const orc_model_ab *m, int which, double *out) {
     case 7: memcpy(out, m->qAc, sizeof(double) * M * m->p.sA); return 0;
     case 8: memcpy(out, m->qBc, sizeof(double) * M * m->p.sB); return 0;
     }
+    return -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Model_ABC: linear A-B-C triblock melt (defined here; the reference has no  */
+/* periodic ABC melt model).  It extends Model_AB term by term:               */
+/*   chain A (sA slices) - B (sB) - C (sC), L = LA + LB + LC, fX = LX / L,    */
+/*   dsX = fX / LX; forward qA -> qB -> qC from 1, complementary qCc -> qBc ->*/
+/*   qAc from 1; Q = mean(qC[sC-1]); phiX = density(ruleX, qX, qXc) / Q;      */
+/*   targets  wA* = xAB phiB + xAC phiC + eta, wB* = xAB phiA + xBC phiC + eta,*/
+/*            wC* = xAC phiA + xBC phiB + eta;                                */
+/*   EM:       eta += lam_eta (phiA + phiB + phiC - 1), wX += lamX (wX* - wX)  */
+/*             (Model_AB.cc:184-193, 254-259 with a third field);             */
+/*   Anderson: eta = (wA + wB + wC - xAB (phiA + phiB) - xBC (phiB + phiC)    */
+/*             - xAC (phiA + phiC)) / 3, the value that makes the targets sum */
+/*             to the current fields (Model_AB's 0.5 (wA + wB - chiN) is the  */
+/*             two-block case with phiA + phiB = 1); one ring per field, one  */
+/*             coefficient set from U = UA + UB + UC, V = VA + VB + VC;       */
+/*   Hw = mean(xAB phiA phiB + xBC phiB phiC + xAC phiA phiC - sum wX phiX),  */
+/*   Hs = -ln Q;  residual as Model_AB's (Anderson: sqrt(sum d^2 / sum w^2);  */
+/*   EM: mean of the three field terms and the incompressibility term).       */
+/* Incompressible, RQM4 only.                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int dim, Lx, Ly, Lz;
+    int s[3];             /* sA, sB, sC */
+    double chi[3];        /* xAB, xBC, xAC (times N) */
+    double lam[4];        /* lamA, lamB, lamC, lamYita */
+    int scft;             /* 0 = EM, 1 = Anderson */
+    int n_anderson;
+    int contour;          /* 0 = trapezoid, 1 = Simpson (Simpson/Quad4 by parity) */
+    const double *k2;     /* -k^2 table (calc_k2_orthogonal), M values */
+} orc_abc_params;
+
+typedef struct {
+    orc_abc_params p;
+    size_t M;
+    double ds[3];
+    int rule[3];
+    orc_updater *up[3];
+    double *q[3], *qc[3];              /* histories: forward and complementary, block X */
+    double *w[3], *yita;               /* EM fields */
+    orc_fieldax ax[3];                 /* Anderson fields */
+    double *phi[3];
+    double Q;
+    double *tgt[3];
+    int last_rc;
+} orc_model_abc;
+
+static const double *abc_w(const orc_model_abc *m, int x) { return m->p.scft == 1 ? m->ax[x].data : m->w[x]; }
+
+orc_model_abc *orc_model_abc_create(const orc_abc_params *p, const double *wA0, const double *wB0,
+                                    const double *wC0) {
+    orc_model_abc *m = (orc_model_abc *)calloc(1, sizeof(orc_model_abc));
+    m->p = *p;
+    size_t M = (size_t)p->Lx * p->Ly * p->Lz;
+    m->M = M;
+    int L[3] = {p->s[0] - 1, p->s[1] - 1, p->s[2] - 1};
+    int Lt = L[0] + L[1] + L[2];
+    const double *w0[3] = {wA0, wB0, wC0};
+    for (int x = 0; x < 3; x++) {
+        double f = 1.0 * L[x] / Lt;
+        m->ds[x] = f / L[x];
+        m->rule[x] = p->contour == 0 ? ORC_TRAPEZOID : ((p->s[x] % 2 != 0) ? ORC_SIMPSON : ORC_QUAD4_CLOSED);
+        m->up[x] = orc_rqm4_create(p->k2, p->Lx, p->Ly, p->Lz, m->ds[x]);
+        m->q[x] = (double *)calloc((size_t)p->s[x] * M, sizeof(double));
+        m->qc[x] = (double *)calloc((size_t)p->s[x] * M, sizeof(double));
+        m->phi[x] = (double *)calloc(M, sizeof(double));
+        m->tgt[x] = (double *)malloc(sizeof(double) * M);
+        if (p->scft == 1) {
+            fax_init(&m->ax[x], p->n_anderson, p->lam[x], M, w0[x]);
+        } else {
+            m->w[x] = (double *)malloc(sizeof(double) * M);
+            memcpy(m->w[x], w0[x], sizeof(double) * M);
+        }
+    }
+    for (size_t i = 0; i < M; i++) { m->q[0][i] = 1.0; m->qc[2][i] = 1.0; }
+    m->yita = (double *)calloc(M, sizeof(double));
+    return m;
+}
+
+void orc_model_abc_destroy(orc_model_abc *m) {
+    if (!m) return;
+    for (int x = 0; x < 3; x++) {
+        orc_updater_destroy(m->up[x]);
+        free(m->q[x]); free(m->qc[x]); free(m->phi[x]); free(m->tgt[x]);
+        if (m->p.scft == 1) fax_free(&m->ax[x]); else free(m->w[x]);
+    }
+    free(m->yita);
+    free(m);
+}
+
+/* the three targets wX* for the current phi and eta */
+static void abc_targets(orc_model_abc *m, const double *eta) {
+    const double xab = m->p.chi[0], xbc = m->p.chi[1], xac = m->p.chi[2];
+    for (size_t i = 0; i < m->M; i++) {
+        double a = m->phi[0][i], b = m->phi[1][i], c = m->phi[2][i];
+        m->tgt[0][i] = xab * b + xac * c + eta[i];
+        m->tgt[1][i] = xab * a + xbc * c + eta[i];
+        m->tgt[2][i] = xac * a + xbc * b + eta[i];
+    }
+}
+
+int orc_model_abc_update(orc_model_abc *m) {
+    size_t M = m->M;
+    const orc_abc_params *p = &m->p;
+    const int *s = p->s;
+    /* forward A -> B -> C */
+    orc_updater_solve(m->up[0], abc_w(m, 0), m->q[0], s[0]);
+    memcpy(m->q[1], m->q[0] + (size_t)(s[0] - 1) * M, sizeof(double) * M);
+    orc_updater_solve(m->up[1], abc_w(m, 1), m->q[1], s[1]);
+    memcpy(m->q[2], m->q[1] + (size_t)(s[1] - 1) * M, sizeof(double) * M);
+    orc_updater_solve(m->up[2], abc_w(m, 2), m->q[2], s[2]);
+    /* complementary C -> B -> A */
+    orc_updater_solve(m->up[2], abc_w(m, 2), m->qc[2], s[2]);
+    memcpy(m->qc[1], m->qc[2] + (size_t)(s[2] - 1) * M, sizeof(double) * M);
+    orc_updater_solve(m->up[1], abc_w(m, 1), m->qc[1], s[1]);
+    memcpy(m->qc[0], m->qc[1] + (size_t)(s[1] - 1) * M, sizeof(double) * M);
+    orc_updater_solve(m->up[0], abc_w(m, 0), m->qc[0], s[0]);
+
+    double Q = orc_mean(m->q[2] + (size_t)(s[2] - 1) * M, M);
+    m->Q = Q;
+    int rc = 0;
+    for (int x = 0; x < 3; x++) rc |= orc_density(m->rule[x], m->q[x], m->qc[x], s[x], M, m->ds[x], 1.0 / Q, m->phi[x]);
+    m->last_rc = rc;
+
+    const double xab = p->chi[0], xbc = p->chi[1], xac = p->chi[2];
+    if (p->scft == 0) {
+        for (size_t i = 0; i < M; i++) m->yita[i] += p->lam[3] * (m->phi[0][i] + m->phi[1][i] + m->phi[2][i] - 1.0);
+        abc_targets(m, m->yita);
+        for (int x = 0; x < 3; x++)
+            for (size_t i = 0; i < M; i++) m->w[x][i] = m->w[x][i] * (1.0 - p->lam[x]) + p->lam[x] * m->tgt[x][i];
+        return rc;
+    }
+    for (size_t i = 0; i < M; i++) {
+        double a = m->phi[0][i], b = m->phi[1][i], c = m->phi[2][i];
+        double sw = m->ax[0].data[i] + m->ax[1].data[i] + m->ax[2].data[i];
+        m->yita[i] = (sw - xab * (a + b) - xbc * (b + c) - xac * (a + c)) / 3.0;
+    }
+    abc_targets(m, m->yita);
+    for (int x = 0; x < 3; x++) fax_pre_update(&m->ax[x], m->tgt[x]);
+    int nn = fax_nn(&m->ax[0]);
+    double U[64 * 64], V[64], C[64];
+    memset(U, 0, sizeof(U)); memset(V, 0, sizeof(V));
+    for (int x = 0; x < 3; x++) fax_add_UV(&m->ax[x], U, V);
+    int nc = 0;
+    if (nn > 0) {
+        if (orc_solve_small(nn, U, V, C) != 0) rc |= 4;
+        nc = nn;
+    }
+    double *W = (double *)malloc(sizeof(double) * M), *D = (double *)malloc(sizeof(double) * M);
+    for (int x = 0; x < 3; x++) fax_update(&m->ax[x], C, nc, W, D);
+    free(W); free(D);
+    return rc;
+}
+
+void orc_model_abc_H(const orc_model_abc *m, double *H, double *Hw, double *Hs) {
+    size_t M = m->M;
+    const double xab = m->p.chi[0], xbc = m->p.chi[1], xac = m->p.chi[2];
+    const double *wa = abc_w(m, 0), *wb = abc_w(m, 1), *wc = abc_w(m, 2);
+    double sum = 0.0;
+    for (size_t i = 0; i < M; i++) {
+        double a = m->phi[0][i], b = m->phi[1][i], c = m->phi[2][i];
+        double g = xab * a * b + xbc * b * c + xac * a * c;
+        g -= wa[i] * a;
+        g -= wb[i] * b;
+        g -= wc[i] * c;
+        sum += g;
+    }
+    double hw = sum / (double)M, hs = -log(m->Q);
+    *Hw = hw; *Hs = hs; *H = hw + hs;
+}
+
+double orc_model_abc_residual(const orc_model_abc *m) {
+    size_t M = m->M;
+    if (m->p.scft == 1) {
+        double e1 = 0.0, e2 = 0.0;
+        for (int x = 0; x < 3; x++) {
+            int pos = m->ax[x].cur + 1; if (pos > m->ax[x].n) pos = 0;
+            const double *d = m->ax[x].d + (size_t)pos * M, *w = m->ax[x].w + (size_t)pos * M;
+            double a1 = 0.0, a2 = 0.0;
+            for (size_t i = 0; i < M; i++) { a1 += d[i] * d[i]; a2 += w[i] * w[i]; }
+            e1 += a1 / (double)M;
+            e2 += a2 / (double)M;
+        }
+        return sqrt(e1 / e2);
+    }
+    /* EM: the targets of the fields after the update (this iteration's phi, eta) */
+    orc_model_abc *mm = (orc_model_abc *)m;
+    abc_targets(mm, m->yita);
+    double res = 0.0;
+    double *g = (double *)malloc(sizeof(double) * M);
+    for (int x = 0; x < 3; x++) {
+        for (size_t i = 0; i < M; i++) g[i] = m->tgt[x][i] - m->w[x][i];
+        res += mean_abs(g, M) / (mean_abs(m->w[x], M) + mean_abs(m->tgt[x], M));
+    }
+    double *t = (double *)malloc(sizeof(double) * M);
+    for (size_t i = 0; i < M; i++) { t[i] = m->phi[0][i] + m->phi[1][i] + m->phi[2][i]; g[i] = t[i] - 1.0; }
+    res += mean_abs(g, M) / (1.0 + mean_abs(t, M));
+    free(g); free(t);
+    return res / 4.0;
+}
+
+double orc_model_abc_Q(const orc_model_abc *m) { return m->Q; }
+
+/* which = 0..2 wA, wB, wC; 3..5 phiA, phiB, phiC; 6 yita */
+int orc_model_abc_get(const orc_model_abc *m, int which, double *out) {
+    size_t M = m->M;
+    if (which >= 0 && which < 3) { memcpy(out, abc_w(m, which), sizeof(double) * M); return 0; }
+    if (which >= 3 && which < 6) { memcpy(out, m->phi[which - 3], sizeof(double) * M); return 0; }
+    if (which == 6) { memcpy(out, m->yita, sizeof(double) * M); return 0; }
     return -1;
 }
 

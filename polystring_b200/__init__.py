@@ -246,6 +246,77 @@ class ModelAB:
             self._h = None
 
 
+ABC_FIELDS = {"wA": 0, "wB": 1, "wC": 2, "phiA": 3, "phiB": 4, "phiC": 5, "yita": 6}
+
+
+def _abc_params(dim, shape, cell, Ms, chi, lam=(0.05, 0.05, 0.05, 5.0), scft="EM", n_anderson=5,
+                contour="Simpson"):
+    """ps_model_abc_params: Ms = (sA, sB, sC), chi = (chiAB, chiBC, chiAC) N,
+    lam = (lamA, lamB, lamC, lamYita)."""
+    p = capi.ModelABCParamsC()
+    p.dim, (p.Lx, p.Ly, p.Lz) = dim, shape
+    p.cell = cell
+    p.sA, p.sB, p.sC = Ms
+    p.chiAB, p.chiBC, p.chiAC = chi
+    p.lamA, p.lamB, p.lamC, p.lamYita = lam
+    p.scft = capi.SCFT[scft.upper()]
+    p.n_anderson = n_anderson
+    p.contour = capi.CONTOUR[contour.upper()]
+    return p
+
+
+class ModelABC:
+    """A linear A-B-C triblock melt on the device (no counterpart in the
+    reference): Model_AB's SCFT iteration with a third block and field,
+    incompressible, RQM4; one iteration is one CUDA graph replay."""
+
+    def __init__(self, dim, shape, cell, Ms, chi, lam=(0.05, 0.05, 0.05, 5.0), scft="EM", n_anderson=5,
+                 contour="Simpson"):
+        p = _abc_params(dim, shape, cell, Ms, chi, lam, scft, n_anderson, contour)
+        h = ctypes.c_void_p()
+        capi.check(lib().ps_model_abc_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.shape = tuple(shape)
+        self.Ms = tuple(Ms)
+
+    def set_fields(self, wA, wB, wC):
+        w = [_f64(x) for x in (wA, wB, wC)]
+        capi.check(lib().ps_model_abc_set_fields(self._h, *[capi.dptr(x) for x in w]))
+        return self
+
+    def update(self, n=1):
+        capi.check(lib().ps_model_abc_update(self._h, int(n)))
+
+    def synchronize(self):
+        capi.check(lib().ps_model_abc_synchronize(self._h))
+
+    def Q(self):
+        q = ctypes.c_double()
+        capi.check(lib().ps_model_abc_Q(self._h, ctypes.byref(q)))
+        return q.value
+
+    def H(self):
+        H, Hw, Hs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        capi.check(lib().ps_model_abc_H(self._h, ctypes.byref(H), ctypes.byref(Hw), ctypes.byref(Hs)))
+        return H.value, Hw.value, Hs.value
+
+    def residual_error(self):
+        r = ctypes.c_double()
+        capi.check(lib().ps_model_abc_residual(self._h, ctypes.byref(r)))
+        return r.value
+
+    def get(self, name):
+        out = np.zeros(self.shape)
+        capi.check(lib().ps_model_abc_get(self._h, ABC_FIELDS[name], capi.dptr(out)))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().ps_model_abc_destroy(h)
+            self._h = None
+
+
 class StringAB:
     """polystring_AB on the device: m images advanced together, one captured
     graph per string iteration (SCFT of every image, arc length, spline
@@ -338,24 +409,39 @@ class BatchAB:
     parameters advanced together (the reference runs such solves one per host
     thread, scft/polystring_AB_backThread.cc).  `solves` is a list of dicts of
     ModelAB's constructor arguments (dim, shape, cell, Ms, chiN, lam, scft,
-    n_anderson, compressible, contour; RQM4 only).  update(n) runs n
-    Model_AB::update iterations of every solve; each line pass of a contour
-    step is one launch over all solves still running."""
+    n_anderson, compressible, contour; RQM4 only).  `triblocks` adds linear
+    ABC solves (dicts of ModelABC's constructor arguments), numbered after
+    the AB solves.  update(n) runs n SCFT iterations of every solve; each line
+    pass of a contour step is one launch over all solves still running."""
 
-    def __init__(self, solves):
-        n = len(solves)
-        arr = (capi.ModelABParamsC * n)()
+    def __init__(self, solves, triblocks=()):
+        n, nq = len(solves), len(triblocks)
+        arr = (capi.ModelABParamsC * max(n, 1))()
+        arq = (capi.ModelABCParamsC * max(nq, 1))()
         self.shapes, self.Ms = [], []
         for i, sv in enumerate(solves):
             arr[i] = _params(**sv)
             self.shapes.append(tuple(sv["shape"]))
             self.Ms.append(tuple(sv["Ms"]))
+        for i, sv in enumerate(triblocks):
+            arq[i] = _abc_params(**sv)
+            self.shapes.append(tuple(sv["shape"]))
+            self.Ms.append(tuple(sv["Ms"]))
         h = ctypes.c_void_p()
-        capi.check(lib().ps_batch_ab_create(arr, n, ctypes.byref(h)))
+        if nq:
+            capi.check(lib().ps_batch_ab_create_mixed(arr, n, arq, nq, ctypes.byref(h)))
+        else:
+            capi.check(lib().ps_batch_ab_create(arr, n, ctypes.byref(h)))
         self._h = h
-        self.n = n
+        self.n = n + nq
+        self.n_ab = n
 
-    def set_fields(self, k, wA, wB):
+    def set_fields(self, k, wA, wB, wC=None):
+        """Fields of solve k: (wA, wB) for an AB solve, (wA, wB, wC) for a triblock."""
+        if k >= self.n_ab:
+            w = [_f64(x) for x in (wA, wB, wC)]
+            capi.check(lib().ps_batch_ab_set_fields_abc(self._h, int(k), *[capi.dptr(x) for x in w]))
+            return
         wA, wB = _f64(wA), _f64(wB)
         capi.check(lib().ps_batch_ab_set_fields(self._h, int(k), capi.dptr(wA), capi.dptr(wB)))
 
@@ -383,6 +469,10 @@ class BatchAB:
 
     def get(self, k, name):
         shape, Ms = self.shapes[k], self.Ms[k]
+        if k >= self.n_ab:
+            out = np.zeros(shape)
+            capi.check(lib().ps_batch_ab_get(self._h, int(k), ABC_FIELDS[name], capi.dptr(out)))
+            return out
         if name in ("qA", "qAc"):
             out = np.zeros((Ms[0],) + shape)
         elif name in ("qB", "qBc"):

@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include")]
 
-SOURCES = ["line_pass.cu", "sweep.cu", "sweep64.cu", "cluster_sweep.cu", "twiddles.cu", "field_kernels.cu", "anderson.cu", "engine.cu", "adjoint.cu", "string_ab.cu", "capi.cu", "density_noalloc.cu", "autotune.cu", "grouped_pass.cu", "batch_ab.cu", "fp64_peak.cu", "etdrk4.cu"]
+SOURCES = ["line_pass.cu", "sweep.cu", "sweep64.cu", "cluster_sweep.cu", "twiddles.cu", "field_kernels.cu", "anderson.cu", "engine.cu", "adjoint.cu", "string_ab.cu", "capi.cu", "density_noalloc.cu", "autotune.cu", "grouped_pass.cu", "batch_ab.cu", "fp64_peak.cu", "etdrk4.cu", "model_abc.cu"]
 
 
 def _headers():

@@ -50,6 +50,15 @@ class ModelABParamsC(ctypes.Structure):
                 ("etdrk4_M", ctypes.c_int)]
 
 
+class ModelABCParamsC(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("Lx", ctypes.c_int), ("Ly", ctypes.c_int), ("Lz", ctypes.c_int),
+                ("cell", UnitCellC), ("sA", ctypes.c_int), ("sB", ctypes.c_int), ("sC", ctypes.c_int),
+                ("chiAB", ctypes.c_double), ("chiBC", ctypes.c_double), ("chiAC", ctypes.c_double),
+                ("lamA", ctypes.c_double), ("lamB", ctypes.c_double), ("lamC", ctypes.c_double),
+                ("lamYita", ctypes.c_double), ("scft", ctypes.c_int), ("n_anderson", ctypes.c_int),
+                ("contour", ctypes.c_int)]
+
+
 SIGNATURES = [
     ("ps_version", ctypes.c_char_p, []),
     ("ps_tuning_log", ctypes.c_char_p, []),
@@ -87,6 +96,15 @@ SIGNATURES = [
     ("ps_model_ab_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     ("ps_model_ab_device_ptr", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ps_model_ab_synchronize", ctypes.c_int, [_vp]),
+    ("ps_model_abc_create", ctypes.c_int, [ctypes.POINTER(ModelABCParamsC), ctypes.POINTER(_vp)]),
+    ("ps_model_abc_destroy", None, [_vp]),
+    ("ps_model_abc_set_fields", ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    ("ps_model_abc_update", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("ps_model_abc_Q", ctypes.c_int, [_vp, _dp]),
+    ("ps_model_abc_H", ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    ("ps_model_abc_residual", ctypes.c_int, [_vp, _dp]),
+    ("ps_model_abc_get", ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    ("ps_model_abc_synchronize", ctypes.c_int, [_vp]),
     ("ps_model_ab_launches_per_iteration", ctypes.c_int, [_vp]),
     ("ps_model_ab_launches_per_propagate", ctypes.c_int, [_vp]),
     ("ps_model_ab_stream", _vp, [_vp]),
@@ -107,6 +125,9 @@ SIGNATURES = [
     ("ps_string_ab_device_ptr", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     ("ps_string_ab_stream", _vp, [_vp]),
     ("ps_batch_ab_create", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ps_batch_ab_create_mixed", ctypes.c_int, [ctypes.POINTER(ModelABParamsC), ctypes.c_int,
+                                                ctypes.POINTER(ModelABCParamsC), ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("ps_batch_ab_set_fields_abc", ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp, _dp]),
     ("ps_batch_ab_destroy", None, [_vp]),
     ("ps_batch_ab_set_fields", ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
     ("ps_batch_ab_update", ctypes.c_int, [_vp, ctypes.c_int]),

@@ -28,7 +28,8 @@ __device__ __forceinline__ int find_index(int cur, int n, int j) {
     return i;
 }
 
-// yita / eta and d(cur) for both fields
+// yita / eta and d(cur) for every field
+template <int NF>
 __global__ void ax_prepare_kernel(AXArgs a) {
     const AXState* s = a.state;
     const int cur = s->cur;
@@ -40,66 +41,75 @@ __global__ void ax_prepare_kernel(AXArgs a) {
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
         double pa = a.phiA[i], pb = a.phiB[i];
-        double y;
-        if (a.compressible) {
-            y = a.lamYita * (pa + pb - 1.0);
+        if constexpr (NF == 2) {
+            double y;
+            if (a.compressible) {
+                y = a.lamYita * (pa + pb - 1.0);
+            } else {
+                y = 0.5 * (a.dataA[i] + a.dataB[i] - a.chiN);
+                a.yita[i] = y;
+            }
+            dA[i] = (a.chiN * pb + y) - wA[i];
+            dB[i] = (a.chiN * pa + y) - wB[i];
         } else {
-            y = 0.5 * (a.dataA[i] + a.dataB[i] - a.chiN);
+            const double pc = a.phiC[i];
+            const double xab = a.chi[0], xbc = a.chi[1], xac = a.chi[2];
+            const double sw = a.dataA[i] + a.dataB[i] + a.dataC[i];
+            const double y = (sw - xab * (pa + pb) - xbc * (pb + pc) - xac * (pa + pc)) / 3.0;
             a.yita[i] = y;
+            dA[i] = (xab * pb + xac * pc + y) - wA[i];
+            dB[i] = (xab * pa + xbc * pc + y) - wB[i];
+            a.dC[(long)cur * M + i] = (xac * pa + xbc * pb + y) - a.wC[(long)cur * M + i];
         }
-        dA[i] = (a.chiN * pb + y) - wA[i];
-        dB[i] = (a.chiN * pa + y) - wB[i];
     }
 }
 
 // partial sums of d(cur) . d(find_index(j)) for j = 4 blockIdx.y .. + 3
-// (both fields); every thread visits the same points i in the same order
+// (every field); every thread visits the same points i in the same order
 // for every j, so the sums do not depend on the split over blockIdx.y
 constexpr int kJC = 4;
 
-template <int NMAX>
+template <int NF, int NMAX>
 __global__ void __launch_bounds__(kRedThreads) ax_dots_kernel(AXArgs a, double* partial) {
     const AXState* s = a.state;
     const int n = s->n, cur = s->cur;
     const int nn = s->k < n ? s->k : n;
     const long M = a.M;
     const int j0 = blockIdx.y * kJC;
-    const double* dcA = a.dA + (long)cur * M;
-    const double* dcB = a.dB + (long)cur * M;
-    double acc[2 * kJC];
+    const double* dF[3] = {a.dA, a.dB, NF == 3 ? a.dC : a.dA};
+    double acc[NF * kJC];
 #pragma unroll
-    for (int j = 0; j < 2 * kJC; j++) acc[j] = 0.0;
+    for (int j = 0; j < NF * kJC; j++) acc[j] = 0.0;
     long kk[kJC];
 #pragma unroll
     for (int j = 0; j < kJC; j++) kk[j] = (long)find_index(cur, n, j0 + j <= nn ? j0 + j : 0) * M;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
-        double xa = dcA[i], xb = dcB[i];
 #pragma unroll
-        for (int j = 0; j < kJC; j++) {
-            if (j0 + j <= nn) {
-                acc[j] += xa * a.dA[kk[j] + i];
-                acc[kJC + j] += xb * a.dB[kk[j] + i];
-            }
+        for (int f = 0; f < NF; f++) {
+            const double x = dF[f][(long)cur * M + i];
+#pragma unroll
+            for (int j = 0; j < kJC; j++)
+                if (j0 + j <= nn) acc[f * kJC + j] += x * dF[f][kk[j] + i];
         }
     }
     // block reduction
-    __shared__ double sh[2 * kJC][kRedThreads / 32];
+    __shared__ double sh[NF * kJC][kRedThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int j = 0; j < 2 * kJC; j++) {
+    for (int j = 0; j < NF * kJC; j++) {
         double v = acc[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) sh[j][warp] = v;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < 2 * kJC; q += blockDim.x) {
-        const int j = j0 + (q % kJC);
+    for (int q = threadIdx.x; q < NF * kJC; q += blockDim.x) {
+        const int f = q / kJC, j = j0 + (q % kJC);
         if (j >= NMAX) continue;
         double t = 0.0;
         for (int w = 0; w < kRedThreads / 32; w++) t += sh[q][w];
-        partial[(long)blockIdx.x * 2 * NMAX + (q < kJC ? 0 : NMAX) + j] = t;
+        partial[(long)blockIdx.x * NF * NMAX + f * NMAX + j] = t;
     }
 }
 
@@ -108,31 +118,31 @@ __global__ void __launch_bounds__(kRedThreads) ax_dots_kernel(AXArgs a, double* 
 // element gets the same operations as in the oracle's orc_solve_small (row i
 // of step k: f = A[i][k] / piv, A[i][j] -= f A[k][j]); the pivot is the first
 // row of largest |A[i][k]|; back substitution runs in order on one thread.
-template <int NMAX>
+template <int NF, int NMAX>
 __global__ void __launch_bounds__(kRedThreads) ax_solve_kernel(AXArgs a, const double* partial, int G) {
     AXState* s = a.state;
     const int n = s->n;
     const int N1 = n + 1;
     const int nn = s->k < n ? s->k : n;
     const int tid = threadIdx.x, nt = blockDim.x;
-    __shared__ double row[2 * NMAX];
-    __shared__ double sB[2][(NMAX + 1) * (NMAX + 1)];
+    __shared__ double row[NF * NMAX];
+    __shared__ double sB[NF][(NMAX + 1) * (NMAX + 1)];
     __shared__ double U[NMAX * NMAX], V[NMAX], C[NMAX], F[NMAX];
     __shared__ int piv_row, singular;
     // fixed-order reduction of the partial sums
-    for (int j = tid; j < 2 * NMAX; j += nt) {
+    for (int j = tid; j < NF * NMAX; j += nt) {
         double t = 0.0;
-        for (int b = 0; b < G; b++) t += partial[(long)b * 2 * NMAX + j];
+        for (int b = 0; b < G; b++) t += partial[(long)b * NF * NMAX + j];
         row[j] = t / (double)a.M;
     }
-    double* BG[2] = {a.BA, a.BB};
-    for (int f = 0; f < 2; f++)
+    double* BG[3] = {a.BA, a.BB, a.BC};
+    for (int f = 0; f < NF; f++)
         for (int e = tid; e < N1 * N1; e += nt) sB[f][e] = BG[f][e];
     if (tid == 0) singular = 0;
     __syncthreads();
     // update_B (FieldAX.cc:321-345): shift the upper triangle down the diagonal
-    double shifted[2][((NMAX + 1) * (NMAX + 1) + kRedThreads - 1) / kRedThreads];
-    for (int f = 0; f < 2; f++) {
+    double shifted[NF][((NMAX + 1) * (NMAX + 1) + kRedThreads - 1) / kRedThreads];
+    for (int f = 0; f < NF; f++) {
         int c = 0;
         for (int e = tid; e < N1 * N1; e += nt, c++) {
             const int i = e / N1, j = e - i * N1;
@@ -140,34 +150,37 @@ __global__ void __launch_bounds__(kRedThreads) ax_solve_kernel(AXArgs a, const d
         }
     }
     __syncthreads();
-    for (int f = 0; f < 2; f++) {
+    for (int f = 0; f < NF; f++) {
         int c = 0;
         for (int e = tid; e < N1 * N1; e += nt, c++) sB[f][e] = shifted[f][c];
     }
     __syncthreads();
-    for (int j = tid; j <= nn; j += nt) {   // new row 0
-        sB[0][j] = row[j];
-        sB[1][j] = row[NMAX + j];
-    }
+    for (int j = tid; j <= nn; j += nt)     // new row 0
+        for (int f = 0; f < NF; f++) sB[f][j] = row[f * NMAX + j];
     __syncthreads();
-    for (int f = 0; f < 2; f++)             // symmetrise
+    for (int f = 0; f < NF; f++)            // symmetrise
         for (int e = tid; e < N1 * N1; e += nt) {
             const int i = e / N1, j = e - i * N1;
             if (j < i) sB[f][e] = sB[f][j * N1 + i];
         }
     __syncthreads();
-    for (int f = 0; f < 2; f++)
+    for (int f = 0; f < NF; f++)
         for (int e = tid; e < N1 * N1; e += nt) BG[f][e] = sB[f][e];
-    // U = UA + UB, V = VA + VB (FieldAX.cc:352-381)
-    const double* BA = sB[0];
-    const double* BB = sB[1];
+    // U = UA + UB (+ UC), V = VA + VB (+ VC) (FieldAX.cc:352-381)
     for (int e = tid; e < nn * nn; e += nt) {
         const int i = e / nn, j = e - i * nn;
-        double ua = BA[0] - BA[(i + 1) * N1] - BA[j + 1] + BA[(i + 1) * N1 + (j + 1)];
-        double ub = BB[0] - BB[(i + 1) * N1] - BB[j + 1] + BB[(i + 1) * N1 + (j + 1)];
-        U[e] = 0.0 + ua + ub;
+        double u = 0.0;
+        for (int f = 0; f < NF; f++) {
+            const double* Bf = sB[f];
+            u = u + (Bf[0] - Bf[(i + 1) * N1] - Bf[j + 1] + Bf[(i + 1) * N1 + (j + 1)]);
+        }
+        U[e] = u;
     }
-    for (int i = tid; i < nn; i += nt) V[i] = 0.0 + (BA[0] - BA[(i + 1) * N1]) + (BB[0] - BB[(i + 1) * N1]);
+    for (int i = tid; i < nn; i += nt) {
+        double v = 0.0;
+        for (int f = 0; f < NF; f++) v = v + (sB[f][0] - sB[f][(i + 1) * N1]);
+        V[i] = v;
+    }
     __syncthreads();
     for (int k = 0; k < nn; k++) {
         if (tid == 0) {
@@ -229,12 +242,26 @@ __global__ void __launch_bounds__(kRedThreads) ax_solve_kernel(AXArgs a, const d
     s->nc = nc;
     s->rampA = 1.0 - pow(s->lamA, (double)(s->k + 1));
     s->rampB = 1.0 - pow(s->lamB, (double)(s->k + 1));
+    if (NF == 3) s->rampC = 1.0 - pow(s->lamC, (double)(s->k + 1));
     s->cur_old = s->cur;
     s->cur_new = s->cur > 0 ? s->cur - 1 : n;
     s->cur = s->cur_new;
     s->k += 1;
 }
 
+// W and D of one field at point i, w(cur') = W + ramp D
+__device__ __forceinline__ double ax_mix(const double* w, const double* d, long oc, long i, const double* C,
+                                         const long* kk, int nc, double ramp) {
+    const double wc = w[oc + i], dc = d[oc + i];
+    double W = wc, D = dc;
+    for (int j = 0; j < nc; j++) {
+        W += C[j] * (w[kk[j] + i] - wc);
+        D += C[j] * (d[kk[j] + i] - dc);
+    }
+    return W + ramp * D;
+}
+
+template <int NF>
 __global__ void ax_combine_kernel(AXArgs a) {
     const AXState* s = a.state;
     const int n = s->n, co = s->cur_old, cn = s->cur_new, nc = s->nc;
@@ -246,24 +273,12 @@ __global__ void ax_combine_kernel(AXArgs a) {
         kk[i] = (long)find_index(co, n, i + 1) * M;
     }
     __syncthreads();
-    const double rA = s->rampA, rB = s->rampB;
+    const double rA = s->rampA, rB = s->rampB, rC = s->rampC;
     const long oc = (long)co * M, on = (long)cn * M;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += stride) {
-        double wc = a.wA[oc + i], dc = a.dA[oc + i];
-        double W = wc, D = dc;
-        for (int j = 0; j < nc; j++) {
-            W += C[j] * (a.wA[kk[j] + i] - wc);
-            D += C[j] * (a.dA[kk[j] + i] - dc);
-        }
-        double na = W + rA * D;
-        wc = a.wB[oc + i]; dc = a.dB[oc + i];
-        W = wc; D = dc;
-        for (int j = 0; j < nc; j++) {
-            W += C[j] * (a.wB[kk[j] + i] - wc);
-            D += C[j] * (a.dB[kk[j] + i] - dc);
-        }
-        double nb = W + rB * D;
+        const double na = ax_mix(a.wA, a.dA, oc, i, C, kk, nc, rA);
+        const double nb = ax_mix(a.wB, a.dB, oc, i, C, kk, nc, rB);
         a.wA[on + i] = na;
         a.wB[on + i] = nb;
         a.dataA[i] = na;
@@ -273,6 +288,15 @@ __global__ void ax_combine_kernel(AXArgs a) {
             a.eHA[i] = exp(-0.25 * a.dsA * na);
             a.eFB[i] = exp(-0.5 * a.dsB * nb);
             a.eHB[i] = exp(-0.25 * a.dsB * nb);
+        }
+        if constexpr (NF == 3) {
+            const double nc3 = ax_mix(a.wC, a.dC, oc, i, C, kk, nc, rC);
+            a.wC[on + i] = nc3;
+            a.dataC[i] = nc3;
+            if (a.eFC) {
+                a.eFC[i] = exp(-0.5 * a.dsC * nc3);
+                a.eHC[i] = exp(-0.25 * a.dsC * nc3);
+            }
         }
     }
 }
@@ -293,28 +317,35 @@ int ax_nmax(int n) {
     return 0;
 }
 
-void launch_anderson(const AXArgs& a, double* partial, cudaStream_t st) {
+template <int NF, int NMAX>
+void launch_ax_nf(const AXArgs& a, double* partial, cudaStream_t st) {
+    ax_dots_kernel<NF, NMAX><<<dim3(kRedBlocks, (NMAX + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
+    ax_solve_kernel<NF, NMAX><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
+}
+
+template <int NF>
+void launch_anderson_nf(const AXArgs& a, double* partial, cudaStream_t st) {
     const int nmax = ax_nmax(a.n);
     if (nmax == 0) throw Error(-2, "Anderson history longer than 31 is not supported");
-    ax_prepare_kernel<<<grid_for(a.M), 256, 0, st>>>(a);
+    ax_prepare_kernel<NF><<<grid_for(a.M), 256, 0, st>>>(a);
     PS_CUDA(cudaGetLastError());
     switch (nmax) {
-    case 8:
-        ax_dots_kernel<8><<<dim3(kRedBlocks, (8 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
-        ax_solve_kernel<8><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
-        break;
-    case 16:
-        ax_dots_kernel<16><<<dim3(kRedBlocks, (16 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
-        ax_solve_kernel<16><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
-        break;
-    default:
-        ax_dots_kernel<32><<<dim3(kRedBlocks, (32 + kJC) / kJC), kRedThreads, 0, st>>>(a, partial);
-        ax_solve_kernel<32><<<1, kRedThreads, 0, st>>>(a, partial, kRedBlocks);
-        break;
+    case 8: launch_ax_nf<NF, 8>(a, partial, st); break;
+    case 16: launch_ax_nf<NF, 16>(a, partial, st); break;
+    default: launch_ax_nf<NF, 32>(a, partial, st); break;
     }
     PS_CUDA(cudaGetLastError());
-    ax_combine_kernel<<<grid_for(a.M), 256, 0, st>>>(a);
+    ax_combine_kernel<NF><<<grid_for(a.M), 256, 0, st>>>(a);
     PS_CUDA(cudaGetLastError());
+}
+
+void launch_anderson(const AXArgs& a, double* partial, cudaStream_t st) {
+    if (a.nf == 3) {
+        if (a.compressible) throw Error(-2, "three-field Anderson mixing is incompressible");
+        launch_anderson_nf<3>(a, partial, st);
+    } else {
+        launch_anderson_nf<2>(a, partial, st);
+    }
 }
 
 }  // namespace ps

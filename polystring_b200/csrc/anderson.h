@@ -21,6 +21,7 @@ struct AXState {
     double lamA, lamB;    // FieldAX::_lambda of A and B
     double rampA, rampB;  // 1 - lambda^(k+1) of the last update
     double C[kAXMaxHist];
+    double lamC, rampC;   // the third field of a triblock (Model_ABC)
 };
 
 struct AXArgs {
@@ -35,10 +36,19 @@ struct AXArgs {
     double chiN, lamYita, dsA, dsB;
     int compressible;
     double *eFA, *eHA, *eFB, *eHB;   // next Boltzmann factors (nullable)
+    // three fields (Model_ABC): nf = 3, field C and the pair interactions
+    // chi = (chiAB, chiBC, chiAC) N; eta = (wA + wB + wC - chiAB (phiA + phiB)
+    // - chiBC (phiB + phiC) - chiAC (phiA + phiC)) / 3 (incompressible only)
+    int nf;                          // 0 or 2: A and B; 3: A, B, C
+    const double* phiC;
+    double *dataC, *wC, *dC, *BC;
+    double dsC;
+    double *eFC, *eHC;
+    double chi[3];
 };
 
 int ax_nmax(int n);
-// partial: kRedBlocks x 64 doubles of scratch
+// partial: kRedBlocks x 64 doubles of scratch (x 96 with three fields)
 void launch_anderson(const AXArgs& a, double* partial, cudaStream_t st);
 
 }  // namespace ps

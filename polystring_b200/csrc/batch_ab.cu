@@ -1,5 +1,7 @@
 // batch_ab.cu -- many independent Model_AB solves, of uneven grid sizes,
-// contour lengths Ns, block fractions, cells and chiN, advanced together.
+// contour lengths Ns, block fractions, cells and chiN, advanced together
+// (with, optionally, linear ABC triblock solves of model_abc.cu, which always
+// take the grouped line passes).
 //
 // The reference runs independent solves one per host thread
 // (scft/polystring_AB_backThread.cc); on one B200 a single small solve
@@ -38,8 +40,8 @@ enum { K_FIRST, K_MID, K_END, K_FWD, K_FWD3, K_INV, K_INV3, K_OUT, K_OUT3 };
 
 }  // namespace
 
-BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
-    if (ps.empty()) throw Error(-1, "a batch needs at least one solve");
+BatchAB::BatchAB(const std::vector<ModelABParams>& ps, const std::vector<ModelABCParams>& qs) {
+    if (ps.empty() && qs.empty()) throw Error(-1, "a batch needs at least one solve");
     grouped_prepare();
     PS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     try {
@@ -52,6 +54,14 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             m_.push_back(new ModelAB(p, true));
             if (m_.back()->chain()->plan().naxes < 2) throw Error(-2, "batched solves need 2D or 3D grids");
         }
+        for (const ModelABCParams& q : qs) {
+            const int sizes[3] = {q.Lx, q.Ly, q.Lz};
+            for (int n : sizes)
+                if (n > 1 && !grouped_size_supported(n))
+                    throw Error(-2, "batched solves support axis lengths 16, 24, 32, 48, 64, 96, 128");
+            t_.push_back(new ModelABC(q));
+            if (t_.back()->chain()->plan().naxes < 2) throw Error(-2, "batched solves need 2D or 3D grids");
+        }
         // persistent sweeps where the grid has one, grouped line passes for the rest
         std::vector<int> swept, passes;
         for (int k = 0; k < (int)m_.size(); k++) {
@@ -59,11 +69,13 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             else if (m_[k]->persistent_sweep()) swept.push_back(k);
             else passes.push_back(k);
         }
+        // triblock solves always take the grouped line passes
+        for (int j = 0; j < (int)t_.size(); j++) passes.push_back((int)m_.size() + j);
         build_sweeps(swept);
         // groups: same number of long axes (the step's pass sequence) and the
         // same schedule on each axis role (one kernel per grouped pass)
         auto key = [&](int k) {
-            const AxisPlan& pl = m_[k]->chain()->plan();
+            const AxisPlan& pl = chain_of(k)->plan();
             return std::array<int, 4>{pl.naxes, pl.ax[0].reg, pl.naxes == 3 ? pl.ax[1].reg : 0,
                                       pl.ax[pl.naxes - 1].reg};
         };
@@ -77,7 +89,7 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps) {
             for (int k : passes)
                 if (key(k) == kk) g.members.push_back(k);
             std::stable_sort(g.members.begin(), g.members.end(),
-                             [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
+                             [&](int a, int b) { return Ns_of(a) > Ns_of(b); });
             build_group(g);
             groups_.push_back(std::move(g));
         }
@@ -100,6 +112,8 @@ void BatchAB::release() {
     }
     for (auto* m : m_) delete m;
     m_.clear();
+    for (auto* m : t_) delete m;
+    t_.clear();
     if (st_) cudaStreamDestroy(st_);
     st_ = nullptr;
 }
@@ -160,27 +174,59 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
     }
 }
 
+PairChain* BatchAB::chain_of(int k) const {
+    return k < (int)m_.size() ? m_[k]->chain() : t_[k - m_.size()]->chain();
+}
+
+int BatchAB::Ns_of(int k) const { return k < (int)m_.size() ? m_[k]->Ns() : t_[k - m_.size()]->Ns(); }
+
+GroupSolve BatchAB::describe(int k) const {
+    const PairChain& c = *chain_of(k);
+    GroupSolve s{};
+    s.naxes = c.plan().naxes;
+    for (int a = 0; a < s.naxes; a++) {
+        s.ax[a] = c.plan().ax[a];
+        s.tw[a] = twiddle_table(s.ax[a].N);
+    }
+    for (int i3 = 0; i3 < 3; i3++) s.z[i3] = c.z(i3);
+    s.u[0] = c.u(0); s.u[1] = c.u(1);
+    s.L1 = c.L1(); s.L2 = c.L2();
+    const int never = 1 << 30;
+    if (k < (int)m_.size()) {
+        const ModelAB& m = *m_[k];
+        s.Ns = m.Ns();
+        s.M = (double)m.M();
+        s.hf = m.hist_f(); s.hc = m.hist_c();
+        // lane f: A then B; lane c: B then A
+        s.swf[0] = m.LA(); s.swf[1] = never;
+        s.swc[0] = m.LB(); s.swc[1] = never;
+        const int of[3] = {0, 1, 1}, oc[3] = {1, 0, 0};
+        for (int i = 0; i < 3; i++) {
+            s.fF[i] = m.factor(1, of[i]); s.fH[i] = m.factor(0, of[i]);
+            s.cF[i] = m.factor(1, oc[i]); s.cH[i] = m.factor(0, oc[i]);
+        }
+    } else {
+        const ModelABC& m = *t_[k - m_.size()];
+        s.Ns = m.Ns();
+        s.M = (double)m.M();
+        s.hf = m.hist_f(); s.hc = m.hist_c();
+        // lane f: A, B, C; lane c: C, B, A
+        s.swf[0] = m.L(0); s.swf[1] = m.L(0) + m.L(1);
+        s.swc[0] = m.L(2); s.swc[1] = m.L(2) + m.L(1);
+        for (int i = 0; i < 3; i++) {
+            s.fF[i] = m.factor(1, i); s.fH[i] = m.factor(0, i);
+            s.cF[i] = m.factor(1, 2 - i); s.cH[i] = m.factor(0, 2 - i);
+        }
+    }
+    return s;
+}
+
 void BatchAB::build_group(Group& g) {
     std::vector<GroupSolve> d(g.members.size());
     for (size_t i = 0; i < g.members.size(); i++) {
-        ModelAB& m = *m_[g.members[i]];
-        PairChain& c = *m.chain();
-        GroupSolve& s = d[i];
-        s.naxes = c.plan().naxes;
-        for (int a = 0; a < s.naxes; a++) {
-            s.ax[a] = c.plan().ax[a];
-            s.tw[a] = twiddle_table(s.ax[a].N);
-        }
-        s.Ns = m.Ns(); s.LA = m.LA(); s.LB = m.LB();
-        s.M = (double)m.M();
-        s.hf = m.hist_f(); s.hc = m.hist_c();
-        for (int i3 = 0; i3 < 3; i3++) s.z[i3] = c.z(i3);
-        s.u[0] = c.u(0); s.u[1] = c.u(1);
-        s.L1 = c.L1(); s.L2 = c.L2();
-        s.eF[0] = m.factor(1, 0); s.eF[1] = m.factor(1, 1);
-        s.eH[0] = m.factor(0, 0); s.eH[1] = m.factor(0, 1);
-        g.Ns.push_back(s.Ns);
-        g.Ns_max = std::max(g.Ns_max, s.Ns);
+        d[i] = describe(g.members[i]);
+        g.Ns.push_back(d[i].Ns);
+        g.Ns_max = std::max(g.Ns_max, d[i].Ns);
     }
     PS_CUDA(cudaMalloc(&g.dev, sizeof(GroupSolve) * d.size()));
     PS_CUDA(cudaMemcpy(g.dev, d.data(), sizeof(GroupSolve) * d.size(), cudaMemcpyHostToDevice));
@@ -240,12 +286,22 @@ void BatchAB::enqueue_iteration() {
         m->enqueue_post(st_);
         launches += m->launches_per_iteration() - m->launches_per_propagate();
     }
+    for (auto* m : t_) {
+        m->enqueue_post(st_);
+        launches += m->launches_post();
+    }
     launches_ = launches;
 }
 
 ModelAB& BatchAB::model(int k) {
-    if (k < 0 || k >= (int)m_.size()) throw Error(-1, "solve index out of range");
+    if (k < 0 || k >= (int)m_.size()) throw Error(-1, "solve index out of range (or not an AB solve)");
     return *m_[k];
+}
+
+ModelABC& BatchAB::model_abc(int k) {
+    const int j = k - (int)m_.size();
+    if (j < 0 || j >= (int)t_.size()) throw Error(-1, "solve index out of range (or not an ABC solve)");
+    return *t_[j];
 }
 
 void BatchAB::set_fields(int k, const double* wA, const double* wB, bool device_ptrs) {
@@ -253,9 +309,16 @@ void BatchAB::set_fields(int k, const double* wA, const double* wB, bool device_
     model(k).set_fields(wA, wB, device_ptrs);
 }
 
+void BatchAB::set_fields_abc(int k, const double* const w[3], bool device_ptrs) {
+    sync();
+    model_abc(k).set_fields(w, device_ptrs);
+}
+
 void BatchAB::update(int n) {
     sync();
     for (auto* m : m_)
+        if (!m->has_fields()) throw Error(-6, "fields of every solve must be set before the batch runs");
+    for (auto* m : t_)
         if (!m->has_fields()) throw Error(-6, "fields of every solve must be set before the batch runs");
     if (!graph_) {
         PS_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
@@ -274,6 +337,7 @@ void BatchAB::update(int n) {
     }
     for (int i = 0; i < n; i++) PS_CUDA(cudaGraphLaunch(graph_, st_));
     for (auto* m : m_) m->advance(n);
+    for (auto* m : t_) m->count_iterations(n);
 }
 
 double BatchAB::update_timed(int n) {
@@ -297,6 +361,7 @@ void BatchAB::sync() { PS_CUDA(cudaStreamSynchronize(st_)); }
 double BatchAB::gridpoint_steps_per_iteration() const {
     double s = 0.0;
     for (auto* m : m_) s += 2.0 * m->Ns() * (double)m->M();
+    for (auto* m : t_) s += 2.0 * m->Ns() * (double)m->M();
     return s;
 }
 

@@ -11,11 +11,15 @@ namespace ps {
 
 class BatchAB {
 public:
-    explicit BatchAB(const std::vector<ModelABParams>& ps);
+    // AB solves are members 0 .. ps.size() - 1, ABC triblock solves follow
+    explicit BatchAB(const std::vector<ModelABParams>& ps, const std::vector<ModelABCParams>& qs = {});
     ~BatchAB();
-    int size() const { return (int)m_.size(); }
+    int size() const { return (int)(m_.size() + t_.size()); }
+    int size_ab() const { return (int)m_.size(); }
     ModelAB& model(int k);
+    ModelABC& model_abc(int k);   // k counts from the first ABC member (k >= size_ab())
     void set_fields(int k, const double* wA, const double* wB, bool device_ptrs);
+    void set_fields_abc(int k, const double* const w[3], bool device_ptrs);
     void update(int n);
     // update() between CUDA events on the batch stream; returns the device ms
     double update_timed(int n);
@@ -43,10 +47,14 @@ private:
         unsigned* bar = nullptr;
     };
     void build_group(Group& g);
+    GroupSolve describe(int k) const;   // grouped-pass descriptor of member k
+    PairChain* chain_of(int k) const;
+    int Ns_of(int k) const;
     void build_sweeps(const std::vector<int>& members);
     void release();
     void enqueue_iteration();
     std::vector<ModelAB*> m_;
+    std::vector<ModelABC*> t_;
     std::vector<Group> groups_;
     std::vector<SweepChunk> chunks_;
     std::vector<int> own_;                   // solves propagated by their own 64^3 sweep

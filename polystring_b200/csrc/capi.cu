@@ -56,6 +56,7 @@ struct ps_updater { UpdaterCtx* ctx; };
 struct ps_model_ab { ModelAB* ctx; };
 struct ps_string_ab { StringAB* ctx; };
 struct ps_batch_ab { BatchAB* ctx; };
+struct ps_model_abc { ModelABC* ctx; };
 
 extern "C" {
 
@@ -172,6 +173,84 @@ static ModelABParams to_params(const ps_model_ab_params* p) {
     q.compressible = p->compressible; q.contour = p->contour;
     q.etd_M = p->etdrk4_M;
     return q;
+}
+
+static ModelABCParams to_abc_params(const ps_model_abc_params* p) {
+    if (!p) throw Error(PS_ERR_INVALID, "null parameters");
+    check_dims(p->dim, p->Lx, p->Ly, p->Lz);
+    if (p->cell.dim != p->dim) throw Error(PS_ERR_INVALID, "cell dimension differs from grid dimension");
+    if (p->scft != PS_SCFT_EM && p->scft != PS_SCFT_ANDERSON) throw Error(PS_ERR_INVALID, "unknown SCFT algorithm");
+    ModelABCParams q;
+    q.dim = p->dim; q.Lx = p->Lx; q.Ly = p->Ly; q.Lz = p->Lz;
+    q.cell = to_cell(&p->cell);
+    q.s[0] = p->sA; q.s[1] = p->sB; q.s[2] = p->sC;
+    q.chi[0] = p->chiAB; q.chi[1] = p->chiBC; q.chi[2] = p->chiAC;
+    q.lam[0] = p->lamA; q.lam[1] = p->lamB; q.lam[2] = p->lamC; q.lam[3] = p->lamYita;
+    q.scft = p->scft; q.n_anderson = p->n_anderson; q.contour = p->contour;
+    return q;
+}
+
+int ps_model_abc_create(const ps_model_abc_params* p, ps_model_abc** out) {
+    return guarded([&] {
+        if (!p || !out) throw Error(PS_ERR_INVALID, "null argument");
+        *out = new ps_model_abc{new ModelABC(to_abc_params(p))};
+    });
+}
+
+void ps_model_abc_destroy(ps_model_abc* m) {
+    if (!m) return;
+    delete m->ctx;
+    delete m;
+}
+
+int ps_model_abc_set_fields(ps_model_abc* m, const double* wA, const double* wB, const double* wC) {
+    return guarded([&] {
+        if (!m || !wA || !wB || !wC) throw Error(PS_ERR_INVALID, "null argument");
+        const double* w[3] = {wA, wB, wC};
+        m->ctx->set_fields(w, false);
+    });
+}
+
+int ps_model_abc_update(ps_model_abc* m, int n_iter) {
+    return guarded([&] {
+        if (!m) throw Error(PS_ERR_INVALID, "null handle");
+        m->ctx->update(n_iter);
+    });
+}
+
+int ps_model_abc_Q(ps_model_abc* m, double* Q) {
+    return guarded([&] {
+        if (!m || !Q) throw Error(PS_ERR_INVALID, "null argument");
+        *Q = m->ctx->Q();
+    });
+}
+
+int ps_model_abc_H(ps_model_abc* m, double* H, double* Hw, double* Hs) {
+    return guarded([&] {
+        if (!m || !H || !Hw || !Hs) throw Error(PS_ERR_INVALID, "null argument");
+        m->ctx->H(H, Hw, Hs);
+    });
+}
+
+int ps_model_abc_residual(ps_model_abc* m, double* res) {
+    return guarded([&] {
+        if (!m || !res) throw Error(PS_ERR_INVALID, "null argument");
+        *res = m->ctx->residual();
+    });
+}
+
+int ps_model_abc_get(ps_model_abc* m, int which, double* out) {
+    return guarded([&] {
+        if (!m || !out) throw Error(PS_ERR_INVALID, "null argument");
+        m->ctx->get(which, out, false);
+    });
+}
+
+int ps_model_abc_synchronize(ps_model_abc* m) {
+    return guarded([&] {
+        if (!m) throw Error(PS_ERR_INVALID, "null handle");
+        PS_CUDA(cudaStreamSynchronize(m->ctx->stream()));
+    });
 }
 
 int ps_model_ab_create(const ps_model_ab_params* p, ps_model_ab** out) {
@@ -395,6 +474,30 @@ int ps_batch_ab_create(const ps_model_ab_params* p, int n, ps_batch_ab** out) {
     });
 }
 
+int ps_batch_ab_create_mixed(const ps_model_ab_params* p, int n, const ps_model_abc_params* q, int nq,
+                             ps_batch_ab** out) {
+    return guarded([&] {
+        if (!out || n < 0 || nq < 0 || n + nq < 1 || (n > 0 && !p) || (nq > 0 && !q))
+            throw Error(PS_ERR_INVALID, "bad batch arguments");
+        std::vector<ModelABParams> ps;
+        std::vector<ModelABCParams> qs;
+        for (int k = 0; k < n; k++) ps.push_back(to_params(p + k));
+        for (int k = 0; k < nq; k++) {
+            qs.push_back(to_abc_params(q + k));
+            if (qs.back().dim < 2) throw Error(PS_ERR_UNSUPPORTED, "batched solves need 2D or 3D grids");
+        }
+        *out = new ps_batch_ab{new BatchAB(ps, qs)};
+    });
+}
+
+int ps_batch_ab_set_fields_abc(ps_batch_ab* b, int k, const double* wA, const double* wB, const double* wC) {
+    return guarded([&] {
+        if (!b || !wA || !wB || !wC) throw Error(PS_ERR_INVALID, "null argument");
+        const double* w[3] = {wA, wB, wC};
+        b->ctx->set_fields_abc(k, w, false);
+    });
+}
+
 void ps_batch_ab_destroy(ps_batch_ab* b) {
     if (!b) return;
     delete b->ctx;
@@ -426,7 +529,8 @@ int ps_batch_ab_H(ps_batch_ab* b, int k, double* H, double* Hw, double* Hs) {
     return guarded([&] {
         if (!b || !H || !Hw || !Hs) throw Error(PS_ERR_INVALID, "null argument");
         b->ctx->sync();
-        b->ctx->model(k).H(H, Hw, Hs);
+        if (k >= b->ctx->size_ab()) b->ctx->model_abc(k).H(H, Hw, Hs);
+        else b->ctx->model(k).H(H, Hw, Hs);
     });
 }
 
@@ -434,7 +538,7 @@ int ps_batch_ab_residual(ps_batch_ab* b, int k, double* res) {
     return guarded([&] {
         if (!b || !res) throw Error(PS_ERR_INVALID, "null argument");
         b->ctx->sync();
-        *res = b->ctx->model(k).residual();
+        *res = k >= b->ctx->size_ab() ? b->ctx->model_abc(k).residual() : b->ctx->model(k).residual();
     });
 }
 
@@ -442,7 +546,8 @@ int ps_batch_ab_get(ps_batch_ab* b, int k, int which, double* out) {
     return guarded([&] {
         if (!b || !out) throw Error(PS_ERR_INVALID, "null argument");
         b->ctx->sync();
-        b->ctx->model(k).get(which, out, false);
+        if (k >= b->ctx->size_ab()) b->ctx->model_abc(k).get(which, out, false);
+        else b->ctx->model(k).get(which, out, false);
     });
 }
 

@@ -54,13 +54,16 @@ void tuning_note(const char* line);   // appends one line to the tuning log
 enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1, SCHEME_ETDRK4 = 2 };
 
 // Which Boltzmann factors a lane uses at step t: set 0 before switch_t,
-// set 1 from switch_t on (a chain crossing the A/B junction).
+// set 1 from switch_t on (a chain crossing the A/B junction); a triblock
+// chain uses set 2 from switch2 on (switch2 > switch_t; 0: two sets).
 struct LaneFactors {
-    const double* eF[2];
-    const double* eH[2];
+    const double* eF[3];
+    const double* eH[3];
     int switch_t;
-    const double* F(int t) const { return t < switch_t ? eF[0] : eF[1]; }
-    const double* H(int t) const { return t < switch_t ? eH[0] : eH[1]; }
+    int switch2;
+    int set(int t) const { return t < switch_t ? 0 : (switch2 > switch_t && t >= switch2 ? 2 : 1); }
+    const double* F(int t) const { return eF[set(t)]; }
+    const double* H(int t) const { return eH[set(t)]; }
 };
 
 // One reverse sweep through a chain of Ns RQM4 steps (adjoint.cu).  Step t
@@ -244,6 +247,65 @@ private:
     bool forward_done_ = false;   // Q, phi of the current fields are valid (forward_only)
     int launches_per_iter_ = 0;
     int launches_per_prop_ = 0;
+};
+
+// Linear A-B-C triblock melt on the device (model_abc.cu; no counterpart in
+// the reference, which has no periodic ABC melt): Model_AB's steps with a
+// third block and field, incompressible, RQM4.  The forward chain A -> B -> C
+// and the complementary chain C -> B -> A share one packed field (three
+// factor sets a lane, two switch steps); propagation runs the line passes.
+struct ModelABCParams {
+    int dim, Lx, Ly, Lz;
+    Cell cell;
+    int s[3];         // Ms of blocks A, B, C
+    double chi[3];    // chiAB, chiBC, chiAC (times N)
+    double lam[4];    // lamA, lamB, lamC, lamYita
+    int scft, n_anderson, contour;
+};
+
+class ModelABC {
+public:
+    explicit ModelABC(const ModelABCParams& p);
+    ~ModelABC();
+    // w: three fields of M values (host or device)
+    void set_fields(const double* const w[3], bool device_ptrs);
+    void update(int n);
+    void enqueue_iteration(cudaStream_t st);   // one iteration on stream st (fields set)
+    double Q();
+    void H(double* H, double* Hw, double* Hs);
+    double residual();
+    // 0..2 wA, wB, wC; 3..5 phiA, phiB, phiC; 6 yita
+    void get(int which, double* out, bool device_dst);
+    int status();
+    long M() const { return M_; }
+    int Ns() const { return Ns_; }
+    int L(int x) const { return L_[x]; }
+    cudaStream_t stream() const { return st_; }
+    void count_iterations(int n) { iter_ += n; }
+    bool has_fields() const { return fields_set_; }
+    // for batches (batch_ab.cu): the packed chain, histories and factors
+    PairChain* chain() const { return chain_; }
+    double* hist_f() const { return hf_.p; }
+    double* hist_c() const { return hc_.p; }
+    const double* factor(int full, int block) const { return full ? eF_[block].p : eH_[block].p; }
+    void enqueue_propagate(cudaStream_t s);
+    void enqueue_post(cudaStream_t s);
+    int launches_post() const { return 2 + 3 + (p_.scft == 1 ? 4 : 1); }
+
+private:
+
+    ModelABCParams p_;
+    long M_;
+    int L_[3], Ns_;
+    double ds_[3];
+    PairChain* chain_ = nullptr;
+    cudaStream_t st_ = nullptr;
+    DevBuf hf_, hc_, w_[3], yita_, phi_[3], eF_[3], eH_[3], c_[3], scal_, partial_;
+    DevBuf hw_[3], hd_[3], B_[3];
+    AXState* axs_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    long iter_ = 0;
+    bool fields_set_ = false;
 };
 
 // Single propagator updater behind the Updater C-ABI (RQM4 / OS2 / ETDRK4)

@@ -121,6 +121,47 @@ struct ResidualAXF {
     }
 };
 
+// Model_ABC (linear ABC triblock): Hw integrand and residual sums, the
+// two-block ones with a third field; chi = (chiAB, chiBC, chiAC) N
+struct HwABCF {
+    const double *phiA, *phiB, *phiC, *wA, *wB, *wC;
+    double xab, xbc, xac;
+    __device__ void operator()(long i, double* v) const {
+        double a = phiA[i], b = phiB[i], c = phiC[i];
+        double g = xab * a * b + xbc * b * c + xac * a * c;
+        g -= wA[i] * a;
+        g -= wB[i] * b;
+        g -= wC[i] * c;
+        v[0] = g;
+    }
+};
+
+// EM branch: per field |w* - w|, |w|, |w*|; then |phiA+phiB+phiC-1|, |phiA+phiB+phiC|
+struct ResidualEMABCF {
+    const double *phiA, *phiB, *phiC, *wA, *wB, *wC, *yita;
+    double xab, xbc, xac;
+    __device__ void operator()(long i, double* v) const {
+        double a = phiA[i], b = phiB[i], c = phiC[i], y = yita[i];
+        double tA = xab * b + xac * c + y;
+        double tB = xab * a + xbc * c + y;
+        double tC = xac * a + xbc * b + y;
+        v[0] = fabs(tA - wA[i]); v[1] = fabs(wA[i]); v[2] = fabs(tA);
+        v[3] = fabs(tB - wB[i]); v[4] = fabs(wB[i]); v[5] = fabs(tB);
+        v[6] = fabs(tC - wC[i]); v[7] = fabs(wC[i]); v[8] = fabs(tC);
+        double t = a + b + c;
+        v[9] = fabs(t - 1.0); v[10] = fabs(t);
+    }
+};
+
+struct ResidualAXABCF {
+    const double *dA, *dB, *dC, *wA, *wB, *wC;
+    __device__ void operator()(long i, double* v) const {
+        v[0] = dA[i] * dA[i]; v[1] = wA[i] * wA[i];
+        v[2] = dB[i] * dB[i]; v[3] = wB[i] * wB[i];
+        v[4] = dC[i] * dC[i]; v[5] = wC[i] * wC[i];
+    }
+};
+
 struct ArcF {
     const double *a, *b;
     __device__ void operator()(long i, double* v) const { double d = a[i] - b[i]; v[0] = d * d; }
@@ -189,6 +230,26 @@ __global__ void em_update_kernel(EMArgs a) {
     }
 }
 
+// Model_ABC simple mixing (incompressible): eta += lam_eta (phiA + phiB +
+// phiC - 1), wX = wX (1 - lamX) + lamX wX*, fused with the next factors
+__global__ void em_update_abc_kernel(EMABCArgs a) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.M; i += stride) {
+        const double pa = a.phi[0][i], pb = a.phi[1][i], pc = a.phi[2][i];
+        const double y = a.yita[i] + a.lam[3] * (pa + pb + pc - 1.0);
+        a.yita[i] = y;
+        const double t[3] = {a.chi[0] * pb + a.chi[2] * pc + y, a.chi[0] * pa + a.chi[1] * pc + y,
+                             a.chi[2] * pa + a.chi[1] * pb + y};
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            const double nw = a.w[x][i] * (1.0 - a.lam[x]) + a.lam[x] * t[x];
+            a.w[x][i] = nw;
+            a.eF[x][i] = exp(-0.5 * a.ds[x] * nw);
+            a.eH[x][i] = exp(-0.25 * a.ds[x] * nw);
+        }
+    }
+}
+
 __global__ void factors_kernel(const double* __restrict__ wA, const double* __restrict__ wB, long M, double dsA,
                                double dsB, double* eFA, double* eHA, double* eFB, double* eHB, long bstride) {
     const long b = blockIdx.y;
@@ -236,6 +297,30 @@ void launch_residual_em(const double* phiA, const double* phiB, const double* wA
 void launch_residual_ax(const double* dA, const double* dB, const double* wA, const double* wB, long M,
                         double* partial, double* out4, cudaStream_t st) {
     reduce_launch<ResidualAXF, 4>(ResidualAXF{dA, dB, wA, wB}, M, partial, out4, 1.0 / (double)M, st);
+}
+
+void launch_Hw_abc(const double* const phi[3], const double* const w[3], const double chi[3], long M,
+                   double* partial, double* out, cudaStream_t st) {
+    reduce_launch<HwABCF, 1>(HwABCF{phi[0], phi[1], phi[2], w[0], w[1], w[2], chi[0], chi[1], chi[2]}, M, partial,
+                             out, 1.0 / (double)M, st);
+}
+
+void launch_residual_em_abc(const double* const phi[3], const double* const w[3], const double* yita,
+                            const double chi[3], long M, double* partial, double* out11, cudaStream_t st) {
+    reduce_launch<ResidualEMABCF, 11>(
+        ResidualEMABCF{phi[0], phi[1], phi[2], w[0], w[1], w[2], yita, chi[0], chi[1], chi[2]}, M, partial, out11,
+        1.0 / (double)M, st);
+}
+
+void launch_residual_ax_abc(const double* const d[3], const double* const w[3], long M, double* partial,
+                            double* out6, cudaStream_t st) {
+    reduce_launch<ResidualAXABCF, 6>(ResidualAXABCF{d[0], d[1], d[2], w[0], w[1], w[2]}, M, partial, out6,
+                                     1.0 / (double)M, st);
+}
+
+void launch_em_update_abc(const EMABCArgs& a, cudaStream_t st) {
+    em_update_abc_kernel<<<grid_for(a.M), 256, 0, st>>>(a);
+    PS_CUDA(cudaGetLastError());
 }
 
 void launch_arc_sq(const double* a, const double* b, long M, double* partial, double* out, cudaStream_t st) {

@@ -50,6 +50,9 @@ __device__ __forceinline__ void dispatch_n(const LineGeom& g, const StepPtrs& p,
     }
 }
 
+// factor set of a lane at step t
+__device__ __forceinline__ int gset(const int* sw, int t) { return t < sw[0] ? 0 : (t < sw[1] ? 1 : 2); }
+
 template <int MODE, int AX, int P3, int PATH>
 __global__ void __launch_bounds__(kThreads, PATH == 2 ? 2 : 1)
     grouped_pass_kernel(const GroupSolve* __restrict__ solves, const int* __restrict__ prefix, int nactive, int t) {
@@ -72,12 +75,14 @@ __global__ void __launch_bounds__(kThreads, PATH == 2 ? 2 : 1)
     p.qout[0] = D.hf + (long)(t + 1) * M;
     p.qin[1] = D.hc + (long)t * M;
     p.qout[1] = D.hc + (long)(t + 1) * M;
-    p.eF[0] = D.eF[t < D.LA ? 0 : 1]; p.eF[1] = D.eF[t < D.LB ? 1 : 0];
-    p.eH[0] = D.eH[t < D.LA ? 0 : 1]; p.eH[1] = D.eH[t < D.LB ? 1 : 0];
+    const int sf = gset(D.swf, t), sc = gset(D.swc, t);
+    p.eF[0] = D.fF[sf]; p.eF[1] = D.cF[sc];
+    p.eH[0] = D.fH[sf]; p.eH[1] = D.cH[sc];
     if (t + 1 < D.Ns) {
         p.chain_next = 1;
-        p.nF[0] = D.eF[t + 1 < D.LA ? 0 : 1]; p.nF[1] = D.eF[t + 1 < D.LB ? 1 : 0];
-        p.nH[0] = D.eH[t + 1 < D.LA ? 0 : 1]; p.nH[1] = D.eH[t + 1 < D.LB ? 1 : 0];
+        const int nf = gset(D.swf, t + 1), nc = gset(D.swc, t + 1);
+        p.nF[0] = D.fF[nf]; p.nF[1] = D.cF[nc];
+        p.nH[0] = D.fH[nf]; p.nH[1] = D.cH[nc];
     }
     p.nfield = P3 ? 1 : 2;
     if (P3) {

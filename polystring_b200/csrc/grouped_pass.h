@@ -7,12 +7,14 @@
 namespace ps {
 
 // One solve of a grouped launch: the paired chains of one Model_AB (lane f:
-// qA -> qB, lane c: qBc -> qAc), its work fields and tables, and its line
-// geometry.  Step t of the solve reads slice t of the histories and writes
-// slice t + 1; lane f is in block A for t < LA, lane c in block B for t < LB.
+// qA -> qB, lane c: qBc -> qAc) or Model_ABC (lane f: qA -> qB -> qC, lane c:
+// qCc -> qBc -> qAc), its work fields and tables, and its line geometry.
+// Step t of the solve reads slice t of the histories and writes slice t + 1;
+// a lane uses its factor set 0 for t < sw[0], set 1 for t < sw[1], then set 2.
 struct GroupSolve {
     LineGeom ax[3];
-    int naxes, Ns, LA, LB;
+    int naxes, Ns;
+    int swf[2], swc[2];         // switch steps of lane f and lane c
     double M;
     double* hf;
     double* hc;
@@ -20,8 +22,10 @@ struct GroupSolve {
     double* u[2];
     const double* L1;
     const double* L2;
-    const double* eF[2];        // e^{-w ds/2} of block A, block B
-    const double* eH[2];        // e^{-w ds/4}
+    const double* fF[3];        // lane f: e^{-w ds/2} of its blocks in chain order
+    const double* fH[3];        // lane f: e^{-w ds/4}
+    const double* cF[3];        // lane c
+    const double* cH[3];
     const double2* tw[3];       // twiddles of each axis
 };
 

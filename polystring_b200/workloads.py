@@ -114,6 +114,30 @@ def uneven_solves(n=27, seed=2024):
     return out
 
 
+def uneven_triblocks(n=64, seed=2025):
+    """The ABC share of C5: linear A-B-C triblock solves on cubic grids
+    {32^3, 48^3, 64^3} with Ns in {64, 128, 256} (cycled like the AB solves),
+    fA ~ U(0.2, 0.5), fB ~ U(0.2, min(0.5, 0.9 - fA)), fC = 1 - fA - fB,
+    chiAB, chiBC, chiAC N ~ U(12, 30), cell ~ U(3.5, 5.0) Rg, Anderson(10),
+    fields 0.1 N(0, 1)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        L = (32, 48, 64)[k % 3]
+        Ns = (64, 128, 256)[(k // 3) % 3]
+        fA = rng.uniform(0.2, 0.5)
+        fB = rng.uniform(0.2, min(0.5, 0.9 - fA))
+        chi = tuple(rng.uniform(12.0, 30.0, 3))
+        a = rng.uniform(3.5, 5.0)
+        shape = (L, L, L)
+        LA, LB = int(round(fA * Ns)), int(round(fB * Ns))
+        Ms = (LA + 1, LB + 1, Ns - LA - LB + 1)
+        w = 0.1 * rng.standard_normal((3,) + shape)
+        out.append(dict(dim=3, shape=shape, cell=("CUBIC", (a,)), Ms=Ms, chi=chi, lam=(0.05, 0.05, 0.05, 5.0),
+                        scft="Anderson", n_anderson=10, w=w))
+    return out
+
+
 def string_images(m=40, shape=(128, 128, 1), L=8.0, seed=2024):
     """C3 initial string: m images linearly interpolated between a lamellar
     and a hexagonal field (polystring_AB.cc:207-214 interpolation)."""
