@@ -1,7 +1,8 @@
 // batch_ab.cu -- many independent Model_AB solves, of uneven grid sizes,
 // contour lengths Ns, block fractions, cells and chiN, advanced together
-// (with, optionally, linear ABC triblock solves of model_abc.cu, which always
-// take the grouped line passes).
+// (with, optionally, linear ABC triblock solves of model_abc.cu, which take
+// the same paths: shared generic sweeps on 32^3 / 48^3 / 64^3 grids, grouped
+// line passes on the others).
 //
 // The reference runs independent solves one per host thread
 // (scft/polystring_AB_backThread.cc); on one B200 a single small solve
@@ -69,8 +70,9 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps, const std::vector<ModelAB
             else if (m_[k]->persistent_sweep()) swept.push_back(k);
             else passes.push_back(k);
         }
-        // triblock solves always take the grouped line passes
-        for (int j = 0; j < (int)t_.size(); j++) passes.push_back((int)m_.size() + j);
+        // triblocks likewise (their grids' generic sweep, else grouped line passes)
+        for (int j = 0; j < (int)t_.size(); j++)
+            (t_[j]->persistent_sweep() ? swept : passes).push_back((int)m_.size() + j);
         build_sweeps(swept);
         // groups: same number of long axes (the step's pass sequence) and the
         // same schedule on each axis role (one kernel per grouped pass)
@@ -124,8 +126,13 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
     // shape -> solves, in member order
     std::map<std::array<int, 3>, std::vector<int>> by_shape;
     for (int k : members) {
-        const ModelABParams& p = m_[k]->params();
-        by_shape[{p.Lx, p.Ly, p.Lz}].push_back(k);
+        if (k < (int)m_.size()) {
+            const ModelABParams& p = m_[k]->params();
+            by_shape[{p.Lx, p.Ly, p.Lz}].push_back(k);
+        } else {
+            const ModelABCParams& p = t_[k - m_.size()]->params();
+            by_shape[{p.Lx, p.Ly, p.Lz}].push_back(k);
+        }
     }
     for (auto& kv : by_shape) {
         const int Lx = kv.first[0], Ly = kv.first[1], Lz = kv.first[2];
@@ -137,7 +144,7 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
         // order of Ns, the launches are consecutive runs of that order; pick
         // the runs with the least total cost (dynamic programme over n).
         std::vector<int> ks = kv.second;
-        std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return m_[a]->Ns() > m_[b]->Ns(); });
+        std::stable_sort(ks.begin(), ks.end(), [&](int a, int b) { return Ns_of(a) > Ns_of(b); });
         const int nk = (int)ks.size();
         auto per_of = [&](int n) { return std::max(1, std::min(tasks, resident / n)); };
         std::vector<double> best(nk + 1, 0.0);
@@ -145,7 +152,7 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
         for (int i = 1; i <= nk; i++) {
             best[i] = -1.0;
             for (int j = std::max(0, i - resident); j < i; j++) {
-                const double c = best[j] + (double)m_[ks[j]]->Ns() * sweep_rounds_per_step(Lx, Ly, Lz, per_of(i - j));
+                const double c = best[j] + (double)Ns_of(ks[j]) * sweep_rounds_per_step(Lx, Ly, Lz, per_of(i - j));
                 if (best[i] < 0.0 || c < best[i]) { best[i] = c; from[i] = j; }
             }
         }
@@ -162,7 +169,8 @@ void BatchAB::build_sweeps(const std::vector<int>& members) {
             PS_CUDA(cudaMalloc(&c.bar, 32 * sizeof(unsigned) * (size_t)c.n));
             std::vector<SweepArgs> d(c.n);
             for (int i = 0; i < c.n; i++) {
-                d[i] = m_[ks[i0 + i]]->sweep_descriptor();
+                const int k = ks[i0 + i];
+                d[i] = k < (int)m_.size() ? m_[k]->sweep_descriptor() : t_[k - m_.size()]->sweep_descriptor();
                 d[i].bar = c.bar + 32 * (size_t)i;
                 d[i].twx = twiddle_table(Lx);
                 d[i].twy = twiddle_table(Ly);

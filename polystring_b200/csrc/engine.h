@@ -55,13 +55,14 @@ enum { SCHEME_RQM4 = 0, SCHEME_OS2 = 1, SCHEME_ETDRK4 = 2 };
 
 // Which Boltzmann factors a lane uses at step t: set 0 before switch_t,
 // set 1 from switch_t on (a chain crossing the A/B junction); a triblock
-// chain uses set 2 from switch2 on (switch2 > switch_t; 0: two sets).
+// chain (eF[2] set) uses set 2 from switch2 on.  switch_t may be negative
+// (a step range that starts past the junction).
 struct LaneFactors {
     const double* eF[3];
     const double* eH[3];
     int switch_t;
     int switch2;
-    int set(int t) const { return t < switch_t ? 0 : (switch2 > switch_t && t >= switch2 ? 2 : 1); }
+    int set(int t) const { return t < switch_t ? 0 : (eF[2] && t >= switch2 ? 2 : 1); }
     const double* F(int t) const { return eF[set(t)]; }
     const double* H(int t) const { return eH[set(t)]; }
 };
@@ -291,6 +292,10 @@ public:
     void enqueue_propagate(cudaStream_t s);
     void enqueue_post(cudaStream_t s);
     int launches_post() const { return 2 + 3 + (p_.scft == 1 ? 4 : 1); }
+    // the generic persistent sweep (32^3, 48^3, 64^3 grids) with three factor sets
+    bool persistent_sweep() const { return use_sweep_; }
+    SweepArgs sweep_descriptor() const;
+    const ModelABCParams& params() const { return p_; }
 
 private:
 
@@ -306,6 +311,11 @@ private:
     cudaGraphExec_t graph_ = nullptr;
     long iter_ = 0;
     bool fields_set_ = false;
+    bool use_sweep_ = false;
+    int sweep_grid_ = 0;
+    DevBuf swZ_, swU_, swL1_, swL2_;
+    unsigned* swbar_ = nullptr;
+    int* swerr_ = nullptr;
 };
 
 // Single propagator updater behind the Updater C-ABI (RQM4 / OS2 / ETDRK4)

@@ -21,9 +21,11 @@
 //     coefficient set from U = UA + UB + UC, V = VA + VB + VC;
 //   * Hw = mean(chiAB phiA phiB + chiBC phiB phiC + chiAC phiA phiC -
 //     sum_X wX phiX), Hs = -ln Q; the residuals of Model_AB with a third field.
-// Incompressible, RQM4, orthogonal k^2 table.  Propagation uses the packed
-// line passes (PairChain) with three factor sets a lane.
+// Incompressible, RQM4, orthogonal k^2 table.  Propagation: the generic
+// persistent sweep (sweep.cu) on 32^3, 48^3 and 64^3 grids, given three
+// factor sets; the packed line passes (PairChain) on other grids.
 #include <cmath>
+#include <cstdlib>
 #include <string>
 
 #include "engine.h"
@@ -62,6 +64,20 @@ ModelABC::ModelABC(const ModelABCParams& p) : p_(p) {
         L2[m] = exp(0.5 * ds_[0] * k2[m]);
     }
     chain_->set_tables(L1, L2);
+    const char* force = getenv("PS_B200_LINE_PASSES");
+    use_sweep_ = !(force && force[0] == '1') && sweep_supported(p.Lx, p.Ly, p.Lz);
+    if (use_sweep_) {
+        sweep_grid_ = sweep_prepare(p.Lx, p.Ly, p.Lz);
+        swZ_.alloc(6 * (size_t)M_);
+        swU_.alloc(2 * (size_t)M_);
+        swL1_.alloc(M_);
+        swL2_.alloc(M_);
+        PS_CUDA(cudaMemcpy(swL1_.p, L1.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMemcpy(swL2_.p, L2.data(), sizeof(double) * M_, cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMalloc(&swbar_, 32 * sizeof(unsigned)));
+        PS_CUDA(cudaMalloc(&swerr_, sizeof(int)));
+        PS_CUDA(cudaMemset(swerr_, 0, sizeof(int)));
+    }
     hf_.alloc((size_t)(Ns_ + 1) * M_);
     hc_.alloc((size_t)(Ns_ + 1) * M_);
     yita_.alloc(M_);
@@ -82,7 +98,7 @@ ModelABC::ModelABC(const ModelABCParams& p) : p_(p) {
     launch_fill(hf_.p, M_, 1.0, st_);
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
-    chain_->autotune(st_);
+    if (!use_sweep_) chain_->autotune(st_);
     PS_CUDA(cudaStreamSynchronize(st_));
 }
 
@@ -90,6 +106,8 @@ ModelABC::~ModelABC() {
     if (graph_) cudaGraphExecDestroy(graph_);
     delete chain_;
     if (axs_) cudaFree(axs_);
+    if (swbar_) cudaFree(swbar_);
+    if (swerr_) cudaFree(swerr_);
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -121,7 +139,26 @@ void ModelABC::set_fields(const double* const w[3], bool dev) {
     fields_set_ = true;
 }
 
+SweepArgs ModelABC::sweep_descriptor() const {
+    if (!use_sweep_) throw Error(-2, "this solve has no generic persistent sweep");
+    SweepArgs a{};
+    a.hf = hf_.p; a.hc = hc_.p;
+    a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
+    a.uf = swU_.p; a.uc = swU_.p + M_;
+    a.eFA = eF_[0].p; a.eHA = eH_[0].p; a.eFB = eF_[1].p; a.eHB = eH_[1].p; a.eFC = eF_[2].p; a.eHC = eH_[2].p;
+    a.L1 = swL1_.p; a.L2 = swL2_.p;
+    a.LA = L_[0]; a.LB = L_[1]; a.LC = L_[2]; a.Ns = Ns_;
+    a.bar = swbar_; a.err = swerr_;
+    return a;
+}
+
 void ModelABC::enqueue_propagate(cudaStream_t s) {
+    if (use_sweep_) {
+        const SweepArgs a = sweep_descriptor();
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), s));
+        sweep_launch(a, p_.Lx, p_.Ly, p_.Lz, sweep_grid_, 1, s, sweep_default_variant(p_.Lx, p_.Ly, p_.Lz));
+        return;
+    }
     // lane f: A for t < LA, B up to LA + LB, then C; lane c: C, B, A
     LaneFactors lf{{eF_[0].p, eF_[1].p, eF_[2].p}, {eH_[0].p, eH_[1].p, eH_[2].p}, L_[0], L_[0] + L_[1]};
     LaneFactors lc{{eF_[2].p, eF_[1].p, eF_[0].p}, {eH_[2].p, eH_[1].p, eH_[0].p}, L_[2], L_[2] + L_[1]};
@@ -255,11 +292,20 @@ void ModelABC::get(int which, double* out, bool device_dst) {
 }
 
 int ModelABC::status() {
-    if (!axs_) return 0;
-    AXState s;
-    PS_CUDA(cudaMemcpyAsync(&s, axs_, sizeof(AXState), cudaMemcpyDeviceToHost, st_));
-    PS_CUDA(cudaStreamSynchronize(st_));
-    return s.status;
+    int st = 0;
+    if (axs_) {
+        AXState s;
+        PS_CUDA(cudaMemcpyAsync(&s, axs_, sizeof(AXState), cudaMemcpyDeviceToHost, st_));
+        PS_CUDA(cudaStreamSynchronize(st_));
+        st |= s.status;
+    }
+    if (swerr_) {
+        int e = 0;
+        PS_CUDA(cudaMemcpyAsync(&e, swerr_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        PS_CUDA(cudaStreamSynchronize(st_));
+        if (e) st |= 2;
+    }
+    return st;
 }
 
 }  // namespace ps

@@ -170,13 +170,19 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, long bidx) {
     double* uc = a.uc + boff;
     const double* L1 = a.L1 + bidx * a.bstride_L;
     const double* L2 = a.L2 + bidx * a.bstride_L;
+    // block (0 A, 1 B, 2 C) of a lane at step t
+    auto block = [&](int lane, int t) -> int {
+        if (!a.eFC) return lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
+        if (lane == 0) return t < a.LA ? 0 : (t < a.LA + a.LB ? 1 : 2);
+        return t < a.LC ? 2 : (t < a.LC + a.LB ? 1 : 0);
+    };
     auto eF = [&](int lane, int t) -> const double* {   // e^{-w ds/2} of the lane's block at step t
-        int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
-        return (blk == 0 ? a.eFA : a.eFB) + boff;
+        const int blk = block(lane, t);
+        return (blk == 0 ? a.eFA : blk == 1 ? a.eFB : a.eFC) + boff;
     };
     auto eH = [&](int lane, int t) -> const double* {
-        int blk = lane == 0 ? (t < a.LA ? 0 : 1) : (t < a.LB ? 1 : 0);
-        return (blk == 0 ? a.eHA : a.eHB) + boff;
+        const int blk = block(lane, t);
+        return (blk == 0 ? a.eHA : blk == 1 ? a.eHB : a.eHC) + boff;
     };
 
     // ---- plane task helpers -------------------------------------------------

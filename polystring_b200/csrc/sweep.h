@@ -21,6 +21,11 @@ struct SweepArgs {
     const double* ktab;              // cluster sweep: per-axis exp(h k_x^2), exp(h k_y^2), h = ds then ds/2
     double2* eHAB;                   // 64^3 sweep: (e^{-w ds/4} of block A, of block B) per point, M
                                      // pairs, written by the sweep's prologue for its x-pass
+    // linear A-B-C triblock (generic sweep only; eFC == nullptr: diblock):
+    // lane f runs A, B, C switching at LA and LA + LB; lane c runs C, B, A
+    // switching at LC and LC + LB
+    const double *eFC, *eHC;
+    int LC;
 };
 
 bool sweep_supported(int Lx, int Ly, int Lz);

@@ -18,3 +18,17 @@ def test_fft_core_all_lengths():
         lines = [l.split() for l in r.stdout.splitlines()]
         assert len(lines) >= 21
         assert max(float(l[2]) for l in lines) < 1e-14
+
+
+def test_lane_factor_sets():
+    """engine.h LaneFactors: the factor set of a packed lane at each step
+    (two-block chains, ranges past the junction, triblock chains)."""
+    src = os.path.join(ROOT, "tests", "native", "lane_factors_check.cpp")
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "lane_factors_check")
+        import shutil
+        nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+        inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "include")
+        subprocess.check_call(["g++", "-O1", "-std=c++17", "-I" + inc, "-o", exe, src])
+        r = subprocess.run([exe], capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr

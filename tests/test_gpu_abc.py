@@ -130,3 +130,21 @@ def test_mixed_batch_members_equal_their_single_solves(ps):
         for f in ("phiA", "phiC", "wB"):
             assert np.array_equal(b.get(k, f), m.get(f)), (k, f)
         assert b.residual_error(k) == m.residual_error()
+
+
+def test_sweep_and_line_passes_agree(ps, monkeypatch):
+    """A 32^3 triblock on the generic persistent sweep (three factor sets a
+    lane) and on the packed line passes (PS_B200_LINE_PASSES=1 at creation)."""
+    shape = (32, 32, 32)
+    w = 0.1 * np.random.default_rng(4).standard_normal((3,) + shape)
+    args = dict(dim=3, shape=shape, cell=ps.make_cell(3, "CUBIC", 4.2), Ms=(31, 25, 29), chi=(16.0, 22.0, 13.0),
+                scft="Anderson", n_anderson=10)
+    a = ps.ModelABC(**args).set_fields(*w)
+    monkeypatch.setenv("PS_B200_LINE_PASSES", "1")
+    b = ps.ModelABC(**args).set_fields(*w)
+    monkeypatch.delenv("PS_B200_LINE_PASSES")
+    a.update(4)
+    b.update(4)
+    assert abs(a.H()[0] - b.H()[0]) < 1e-12 * abs(b.H()[0])
+    for f in ("phiA", "phiB", "phiC"):
+        assert np.abs(a.get(f) - b.get(f)).max() < 1e-12
