@@ -135,3 +135,38 @@ def test_etdrk4_lam1d_example_matches_oracle(ps, golden):
     print("ETDRK4 1D LAM a = 3.0: H %.10f (oracle %.10f), published %.10f, gap %.2e, residual %.2e"
           % (Hg, Ho, golden["1d_etdrk4_F"][i], gap, m.residual_error()))
     assert 0 < gap < 3e-5
+
+
+def test_sech_well_all_three_schemes(ps):
+    """The reference's scheme cross-check (tests/test_rqm4.cc: 1D sech^2 well,
+    Lx 32, cell 10, Ns 101, ETDRK4 with M = 16): the device RQM4, OS2 and
+    ETDRK4 updaters equal the oracle's to 1e-12, and converge at their orders
+    (4, 2, 4) towards the same tail."""
+    lx, Lx = 10.0, 32
+    x = np.linspace(lx / Lx, lx, Lx)
+    w = (1.0 - 2.0 / np.cosh(0.75 * (2.0 * x - lx)) ** 2).reshape(Lx, 1, 1)
+    cell = ps.make_cell(1, "LAMELLAR", lx)
+    k2 = oracle.k2_orthogonal(1, (lx,), w.shape)
+    g = np.diag([2 * np.pi / lx, 2 * np.pi, 2 * np.pi])
+
+    def run(scheme, ds):
+        n = int(round(1.0 / ds)) + 1
+        qs = np.zeros((n,) + w.shape)
+        qs[0] = 1.0
+        if scheme == "RQM4":
+            dev, ora = ps.RQM4(cell, Lx, 1, 1, ds), oracle.Updater("RQM4", k2, w.shape, ds)
+        elif scheme == "OS2":
+            dev = ps.PseudoSpectral(cell, Lx, 1, 1, ds)
+            ora = oracle.Updater("OS2", oracle.k_laplacian(g, w.shape, ds), w.shape, ds)
+        else:
+            dev, ora = ps.Etdrk4_PBC(cell, Lx, 1, 1, ds, M=16), oracle.Updater("ETDRK4", k2, w.shape, ds, Mc=16)
+        a = dev.solve(qs.copy(), w)
+        b = ora.solve(w, qs.copy())
+        assert _rel(a, b) < 1e-12, (scheme, ds, _rel(a, b))
+        return a[-1]
+
+    ref = run("RQM4", 1.0 / 3200)
+    for scheme, order in (("RQM4", 4), ("ETDRK4", 4), ("OS2", 2)):
+        errs = [np.abs(run(scheme, ds) - ref).max() for ds in (0.02, 0.01, 0.005)]
+        rates = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+        assert all(abs(r - order) < 0.35 for r in rates), (scheme, errs, rates)
