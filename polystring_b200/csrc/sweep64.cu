@@ -187,21 +187,21 @@ __device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zo
     double2 v[8];
     double hf[8], hc[8];
 #pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = Zin[(long)(t + 8 * j) * P64 + c];
+    line_op(v, t, scratch, 1, tw, ktab(tab, full ? 0 : 1, 0));
+    // the factors after the first operator: fewer registers live across it
+#pragma unroll
     for (int j = 0; j < 8; j++) {
-        const long g = (long)(t + 8 * j) * P64 + c;
-        v[j] = Zin[g];
-        const double2 e = __ldg(eAB + g);
+        const double2 e = __ldg(eAB + (long)(t + 8 * j) * P64 + c);
         hf[j] = fB ? e.y : e.x;
         hc[j] = cB ? e.y : e.x;
     }
     if (full) {
-        line_op(v, t, scratch, 1, tw, ktab(tab, 0, 0));
 #pragma unroll
         for (int j = 0; j < 8; j++)
             Zout[(long)(t + 8 * j) * P64 + c] =
                 make_double2((v[j].x * (hf[j] * hf[j])) * rMd, (v[j].y * (hc[j] * hc[j])) * rMd);
     } else {
-        line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const double qf = (v[j].x * hf[j]) * rMd, qc = (v[j].y * hc[j]) * rMd;
