@@ -182,17 +182,25 @@ __device__ __forceinline__ void line_op(double2 (&v)[8], int t, double2* line, i
 // and lane c are in block B at this step.  One 16-byte load gives both lanes'
 // factors of a point.
 __device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zout, const double2* eAB,
-                                      bool fB, bool cB, double2* scratch, int c, int t, const double2* tw,
-                                      const double* tab, double rMd) {
+                                      bool fB, bool cB, double2* scratch, double2* estage, int c, int t,
+                                      const double2* tw, const double* tab, double rMd) {
     double2 v[8];
     double hf[8], hc[8];
-#pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = Zin[(long)(t + 8 * j) * P64 + c];
-    line_op(v, t, scratch, 1, tw, ktab(tab, full ? 0 : 1, 0));
-    // the factors after the first operator: fewer registers live across it
+    // the factors travel to this lane's staging slots (estage[32 j]) by
+    // asynchronous copies while the first operator runs: no registers held
 #pragma unroll
     for (int j = 0; j < 8; j++) {
-        const double2 e = __ldg(eAB + (long)(t + 8 * j) * P64 + c);
+        v[j] = Zin[(long)(t + 8 * j) * P64 + c];
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(estage + 32 * j)),
+                     "l"(eAB + (long)(t + 8 * j) * P64 + c)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    line_op(v, t, scratch, 1, tw, ktab(tab, full ? 0 : 1, 0));
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const double2 e = estage[32 * j];
         hf[j] = fB ? e.y : e.x;
         hc[j] = cB ? e.y : e.x;
     }
@@ -302,6 +310,7 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     const int nwarps = gridDim.x * (NT / 32);
     const int lane = tid & 31, cq = lane >> 3;
     double2* scratch = plane + (tid >> 5) * 256 + cq * 64;
+    double2* estage = su + (tid >> 5) * 256 + lane;   // x-pass factor staging (su is idle then)
     double2* ug = reinterpret_cast<double2*>(a.uf);   // interleaved (u_f, u_c)
 
     // lane block at step t: lane f is in A for t < LA, lane c in B for t < LB
@@ -343,8 +352,8 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
         for (int task = gwarp; task < 2 * (P64 / 4); task += nwarps) {
             const bool full = task >= P64 / 4;
             const int c = (full ? task - P64 / 4 : task) * 4 + cq;
-            xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, a.eHAB, st >= a.LA, st < a.LB, scratch, c, t, tw, tab,
-                  rMd);
+            xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, a.eHAB, st >= a.LA, st < a.LB, scratch, estage, c, t,
+                  tw, tab, rMd);
         }
         if (!grid_sync(ctr, a.err, ++bidx)) return;
 
