@@ -227,14 +227,16 @@ __device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zo
 // y = t + 8 j) -> z-line order (row y = r, z = t + 8 j).  One CTA barrier
 // for the transpose through the plane buffer; a second one before the
 // caller reuses the buffer.
+template <class MID>
 __device__ __forceinline__ void slab_yz(double2 (&v)[8], double2* plane, int r, int t, const double2* tw,
-                                        const double* tab, int half) {
+                                        const double* tab, int half, MID&& mid) {
     double2* col = plane + r;
     line_op(v, t, col, PITCH, tw, ktab(tab, half, 1));
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < 8; j++) col[(t + 8 * j) * PITCH] = v[j];
     __syncthreads();
+    mid();   // every thread's loads before the operator are done here
     double2* row = plane + r * PITCH;
 #pragma unroll
     for (int j = 0; j < 8; j++) v[j] = row[8 * j + t];
@@ -360,12 +362,6 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
         // ---- plane: Z3 -> q[st+1] -> next Z1 / Z2 ------------------------------
         const bool next = st + 1 < a.Ns;
         if (planar && (role == 0 || next)) {
-            if (tid == 0) {
-                // order earlier generic-proxy accesses (other CTAs' u stores,
-                // this CTA's reads of su) before the async-proxy bulk copy
-                asm volatile("fence.proxy.async;" ::: "memory");
-                bulk_load(su, ug + soff, P64 * 16, mbar);
-            }
             const double* ef = sh_f(st);
             const double* ec = sh_c(st);
             double2 v[8];
@@ -373,7 +369,17 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
             const double2* Z3 = a.Z3 + soff;
 #pragma unroll
             for (int j = 0; j < 8; j++) v[j] = Z3[(8 * j + t) * 64 + r];
-            slab_yz(v, plane, r, t, tw, tab, 1);
+            // u's bulk copy starts once the Z3 loads are done (they share L2
+            // bandwidth; u is needed only after Dy Dz)
+            slab_yz(v, plane, r, t, tw, tab, 1, [&] {
+                if (tid == 0) {
+                    // order earlier generic-proxy accesses (other CTAs' u stores,
+                    // this CTA's reads and staging writes of su) before the
+                    // async-proxy bulk copy
+                    asm volatile("fence.proxy.async;" ::: "memory");
+                    bulk_load(su, ug + soff, P64 * 16, mbar);
+                }
+            });
             if (!mbar_wait(mbar, mphase)) { atomicExch(a.err, 3); }
             mphase ^= 1u;
             double* of = a.hf + (long)(st + 1) * M64 + soff;
