@@ -231,7 +231,7 @@ private:
     bool use_sweep64_ = false;
     int sweep_grid_ = 0;
     int sweep_variant_ = 0;              // x-tile variant of the generic sweep (tune_sweep)
-    DevBuf swZ_, swU_, swL1_, swL2_, swTab_, swE_;
+    DevBuf swZ_, swU_, swL1_, swL2_, swTab_;
     unsigned* swbar_ = nullptr;
     int* swerr_ = nullptr;
     cudaStream_t st_ = nullptr;

@@ -19,8 +19,6 @@ struct SweepArgs {
     long bstride_hist;               // per-problem stride of the histories
     long bstride_L;                  // per-problem stride of the k tables (0: shared)
     const double* ktab;              // cluster sweep: per-axis exp(h k_x^2), exp(h k_y^2), h = ds then ds/2
-    double2* eHAB;                   // 64^3 sweep: (e^{-w ds/4} of block A, of block B) per point, M
-                                     // pairs, written by the sweep's prologue for its x-pass
     // linear A-B-C triblock (generic sweep only; eFC == nullptr: diblock):
     // lane f runs A, B, C switching at LA and LA + LB; lane c runs C, B, A
     // switching at LC and LC + LB
@@ -32,6 +30,8 @@ bool sweep_supported(int Lx, int Ly, int Lz);
 // 64^3 specialisation (sweep64.cu); bar needs 64 zeroed words, uf holds the
 // interleaved (u_f, u_c) pairs (2 M doubles); tables = 6 x 64 per-axis k factors
 bool sweep64_supported(int Lx, int Ly, int Lz);
+// sets kernel attributes, builds twiddles; returns the grid (two-CTA clusters,
+// one CTA per SM), or 0 when too few clusters can be resident on this device
 int sweep64_prepare();
 void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStream_t st);
 // sets kernel attributes, builds twiddles; returns the cooperative grid size
