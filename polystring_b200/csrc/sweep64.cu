@@ -518,11 +518,13 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     if (planar) cluster_sync_all();   // no peer reads this CTA's shared memory after it exits
 }
 
-// An empty kernel launched once with a cluster dimension and the cooperative
-// attribute: whether this driver accepts the two together.
-__global__ void coop_cluster_probe_kernel(int) {}
-
-cudaLaunchConfig_t sweep64_config(int grid, cudaStream_t st, cudaLaunchAttribute* attr, bool coop) {
+// Launch configuration: two-CTA clusters, one CTA per SM.  The grid barriers
+// need every CTA resident at once; sweep64_prepare sizes the grid by
+// cudaOccupancyMaxActiveClusters, and a barrier that waits too long ends the
+// sweep with an error instead of spinning on.  (The cooperative launch
+// attribute is not combined with the cluster dimension: profilers refuse such
+// launches.)
+cudaLaunchConfig_t sweep64_config(int grid, cudaStream_t st, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
     cfg.blockDim = dim3(NT, 1, 1);
@@ -532,14 +534,10 @@ cudaLaunchConfig_t sweep64_config(int grid, cudaStream_t st, cudaLaunchAttribute
     attr[0].val.clusterDim.x = 2;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    attr[1].id = cudaLaunchAttributeCooperative;
-    attr[1].val.cooperative = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = coop ? 2 : 1;
+    cfg.numAttrs = 1;
     return cfg;
 }
-
-int g_coop_cluster = -1;   // 1: cooperative cluster launches accepted (probed once)
 
 }  // namespace
 
@@ -550,8 +548,8 @@ int sweep64_prepare() {
     int dev = 0, sms = 0;
     PS_CUDA(cudaGetDevice(&dev));
     PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    cudaLaunchAttribute attr[2];
-    cudaLaunchConfig_t cfg = sweep64_config(sms & ~1, nullptr, attr, false);
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = sweep64_config(sms & ~1, nullptr, attr);
     int nclusters = 0;
     PS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, sweep64_kernel, &cfg));
     nclusters = std::min(nclusters, sms / 2);
@@ -559,19 +557,9 @@ int sweep64_prepare() {
     // factors resident, so the 2048 tasks need one warp each among the first
     // XW warps of every CTA
     if (nclusters < 64 || 2 * nclusters * XW < 2 * (P64 / 4)) return 0;
-    if (g_coop_cluster < 0) {
-        cudaLaunchAttribute pa[2];
-        cudaLaunchConfig_t pc = sweep64_config(2, nullptr, pa, true);
-        pc.blockDim = dim3(32, 1, 1);
-        pc.dynamicSmemBytes = 0;
-        cudaError_t e = cudaLaunchKernelEx(&pc, coop_cluster_probe_kernel, 0);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
-        if (e != cudaSuccess) (void)cudaGetLastError();   // a refused launch configuration is not sticky
-        g_coop_cluster = e == cudaSuccess ? 1 : 0;
-    }
     char line[160];
-    std::snprintf(line, sizeof(line), "64^3 sweep: %d clusters of 2 CTAs resident, grid %d, cooperative launch %s\n",
-                  nclusters, 2 * nclusters, g_coop_cluster ? "yes" : "no");
+    std::snprintf(line, sizeof(line), "64^3 sweep: %d clusters of 2 CTAs resident, grid %d\n", nclusters,
+                  2 * nclusters);
     tuning_note(line);
     twiddle_table(64);
     return 2 * nclusters;
@@ -580,8 +568,8 @@ int sweep64_prepare() {
 void sweep64_launch(const SweepArgs& a0, const double* tables, int grid, cudaStream_t st) {
     SweepArgs a = a0;
     a.twx = a.twy = a.twz = twiddle_table(64);
-    cudaLaunchAttribute attr[2];
-    cudaLaunchConfig_t cfg = sweep64_config(grid, st, attr, g_coop_cluster == 1);
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = sweep64_config(grid, st, attr);
     PS_CUDA(cudaLaunchKernelEx(&cfg, sweep64_kernel, a, tables));
 }
 
