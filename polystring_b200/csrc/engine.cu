@@ -434,7 +434,6 @@ ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
     use_sweep_ = allow && p.mde == 0 && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
     if (use_sweep64_) {
         swZ_.alloc(6 * (size_t)M_);
-        swU_.alloc(2 * (size_t)M_);
         // per-axis factors exp(h cc_axis r^2), h = ds (full) and ds/2 (half)
         const double PI = 3.14159265358979323846;
         std::vector<double> tab(6 * 64);
@@ -634,7 +633,6 @@ void ModelAB::enqueue_propagate(cudaStream_t s) {
         SweepArgs a{};
         a.hf = hf_.p; a.hc = hc_.p;
         a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
-        a.uf = swU_.p; a.uc = nullptr;
         a.eFA = eFA_.p; a.eHA = eHA_.p; a.eFB = eFB_.p; a.eHB = eHB_.p;
         a.LA = LA_; a.LB = LB_; a.Ns = Ns_;
         a.bar = swbar_; a.err = swerr_;

@@ -27,8 +27,8 @@ struct SweepArgs {
 };
 
 bool sweep_supported(int Lx, int Ly, int Lz);
-// 64^3 specialisation (sweep64.cu); bar needs 64 zeroed words, uf holds the
-// interleaved (u_f, u_c) pairs (2 M doubles); tables = 6 x 64 per-axis k factors
+// 64^3 specialisation (sweep64.cu); uses hf, hc, Z1-Z3, eHA, eHB, LA, LB,
+// Ns, bar (64 zeroed words) and err; tables = 6 x 64 per-axis k factors
 bool sweep64_supported(int Lx, int Ly, int Lz);
 // sets kernel attributes, builds twiddles; returns the grid (two-CTA clusters,
 // one CTA per SM), or 0 when too few clusters can be resident on this device

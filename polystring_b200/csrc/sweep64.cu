@@ -20,14 +20,15 @@
 // The grid is made of two-CTA thread-block clusters, one CTA per SM.  In the
 // plane phase cluster s < 64 owns slab x = s for the whole sweep, and CTA c of
 // the pair owns the columns z and the rows y in [32 c, 32 c + 32): it runs
-// Dy on its columns, reads its rows from both CTAs' shared memory (DSMEM)
-// after a cluster barrier, runs Dz, combines, writes the history and forms
-// both next inputs of its rows, runs Dz on them, and after a second cluster
-// barrier reads its columns of both from both CTAs and runs Dy.  So every
-// line operator of the plane phase runs once, on half the lines a CTA.  The
-// CTA keeps its rows' e^{-w ds/4} factors of both blocks in shared memory for
-// the whole sweep and prefetches its rows of the full-step result u with a 1D
-// bulk copy (cp.async.bulk, no multicast) completed on an mbarrier.
+// Dy on its columns of the half-step field Z3 and of the full-step field W,
+// reads its rows of both from both CTAs' shared memory (DSMEM) after a
+// cluster barrier, runs Dz on Z3, combines, writes the history and forms both
+// next inputs of its rows, runs Dz on them (W is stored then; its Dx and Dy
+// follow in the next x-pass and plane phase), and after a second cluster
+// barrier reads its columns of the half-step input from both CTAs and runs
+// Dy.  So every line operator of the plane phase runs once, on half a slab a
+// CTA.  The CTA keeps its rows' e^{-w ds/4} factors of both blocks in shared
+// memory for the whole sweep, and so does each x-pass warp for its columns.
 // e^{-w ds/2} is formed as (e^{-w ds/4})^2, and the k-space factors as
 // per-axis tables; both agree with the reference's direct exp() evaluations
 // to a few ulps.
@@ -54,17 +55,19 @@ constexpr int NT = 512;
 constexpr long long kSpin = 20000000;
 
 // shared memory map (bytes)
-//   RA: the two next inputs of the CTA's 32 rows after Dz (row pitch QP),
-//       read by both CTAs for Dy; Dz exchange areas
-//   RB: Z3 after Dy, the CTA's 32 columns (64 rows of pitch PB), read by both
-//       CTAs for Dz, and behind it the CTA's rows of u (bulk copy); the Dy
-//       exchange areas of the next inputs (64 lines, slot pitch SP); x-pass
-//       exchange areas
-//   FC: the x-pass factors of each warp's four columns, loaded in the first
-//       x-pass and kept for the sweep (a warp's task is the same every step)
+//   RA: rows of pitch QP: Dz exchange areas of both fields (rows 0-31 the
+//       full-step field, 32-63 the half-step one), the half-step input after
+//       Dz, read by both CTAs for Dy; Dy exchange areas of the full-step field
+//   RB: Z3 after Dy, the CTA's 32 columns (64 rows of pitch PB), and behind
+//       it the full-step result after Dy, the CTA's 32 columns (64 rows of 32,
+//       swizzled), both read by both CTAs for the rows; the Dy exchange areas
+//       of the half-step input (32 lines, slot pitch SP); x-pass exchange areas
+//   FC: the factors of the four columns of each warp with a half-step x-pass
+//       task, for the whole sweep (a warp's task is the same every step)
 constexpr int QP = 65;                                         // complex
 constexpr int PB = 33;
 constexpr int SP = 65;
+constexpr int UC = 64 * PB;                                    // RB offset of the full-step columns
 constexpr int OFF_RA = 0;
 constexpr int SZ_RA = 2 * 32 * QP * 16;
 constexpr int OFF_RB = OFF_RA + SZ_RA;
@@ -75,17 +78,16 @@ constexpr int SZ_RB = 64 * SP * 16;
 constexpr int EHP = 72;
 constexpr int OFF_EHA = OFF_RB + SZ_RB;                        // 32 x EHP double
 constexpr int OFF_EHB = OFF_EHA + 32 * EHP * 8;
-constexpr int OFF_U = OFF_RB + 64 * PB * 16;                   // 2048 double2 behind the Z3 columns
 constexpr int XW = 14;                                         // x-pass warps a CTA with a task (2048 tasks)
-constexpr int OFF_FC = OFF_EHB + 32 * EHP * 8;                 // XW x 256 double2
-constexpr int OFF_TW = OFF_FC + XW * 256 * 16;                 // 64 double2
+constexpr int XH = 7;                                          // of them with a half-step task (1024 tasks)
+constexpr int OFF_FC = OFF_EHB + 32 * EHP * 8;                 // XH x 256 double2
+constexpr int OFF_TW = OFF_FC + XH * 256 * 16;                 // 64 double2
 constexpr int OFF_TAB = OFF_TW + 64 * 16;                      // 6 x 64 double: x,y,z tables for L1 then L2
-constexpr int OFF_MBAR = OFF_TAB + 6 * 64 * 8;                 // mbarrier (8 B)
-constexpr int OFF_STOP = OFF_MBAR + 8;                         // grid barriers no longer waited (int)
-constexpr int SMEM64 = OFF_MBAR + 16;
-static_assert(64 * PB * 16 + H64 * 16 <= SZ_RB, "Z3 columns and u fit in RB");
-static_assert(16 * 256 * 16 <= SZ_RB, "x-pass scratch fits");
-static_assert(OFF_U % 16 == 0 && OFF_FC % 16 == 0 && OFF_MBAR % 8 == 0, "alignment");
+constexpr int OFF_STOP = OFF_TAB + 6 * 64 * 8;                 // grid barriers no longer waited (int)
+constexpr int SMEM64 = OFF_STOP + 16;
+static_assert((UC + H64) * 16 <= SZ_RB, "Z3 and full-step columns fit in RB");
+static_assert(16 * 256 * 16 <= SZ_RB && (31 + 63 * SP + 1) * 16 <= SZ_RB, "exchange areas fit in RB");
+static_assert(OFF_FC % 16 == 0 && OFF_STOP % 8 == 0, "alignment");
 static_assert(SMEM64 <= 232448, "shared memory of one CTA");
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -123,34 +125,8 @@ __device__ __forceinline__ void grid_sync(unsigned* ctr, int* err, unsigned idx,
     __syncthreads();
 }
 
-// ---- mbarrier + bulk copy (global -> shared) -----------------------------
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(void* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, void* bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-// bounded wait on the mbarrier phase; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(void* bar, unsigned parity) {
-    unsigned ok = 0;
-    long long spins = 0;
-    while (!ok) {
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(ok)
-            : "r"(smem_u32(bar)), "r"(parity)
-            : "memory");
-        if (++spins > kSpin) return false;
-    }
-    return true;
 }
 
 // ---- 64-point four-step FFT, 8 lanes per line ----------------------------
@@ -217,47 +193,46 @@ __device__ __forceinline__ void line_op(double2 (&v)[8], int t, double2* line, i
 __device__ __forceinline__ long xq(int x, int y, int z) { return ((long)((y << 4) + (z >> 2)) * 64 + x) * 4 + (z & 3); }
 
 // x-pass task of 4 columns c = (y, z) (8 lanes a column, lane t holds the
-// stride-8 set x = t + 8 j).
-//   Z1 columns: Dx of the full step, then u = e^{-w ds/2} v / M  -> ug
-//   Z2 columns: Dx of the half step, qt = e^{-w ds/4} v / M, the second half
-//               step's input e^{-w ds/4} qt and its Dx                -> Z3
-// Zin and Z3 are in the x-pass layout (xcol: element x = t of column c; + 32 j
-// for x = t + 8 j), u in natural order.  fc[32 j]: this lane's slots of the
-// warp's factor cache, (e^{-w ds/4} of block A, of block B) of point x = t + 8 j
-// (filled by the kernel's prologue); fB, cB: whether lane f and lane c are in
-// block B at this step.
+// stride-8 set x = t + 8 j), fields in the x-pass layout (xcol: element x = t
+// of column c; + 32 j for x = t + 8 j).
+//   full step (Z1, in place): Dx of the full step (Dz came before, Dy and the
+//               factor e^{-w ds/2} / M follow in the plane phase)
+//   half step (Z2 -> Z3): Dx of the half step, qt = e^{-w ds/4} v / M, the
+//               second half step's input e^{-w ds/4} qt and its Dx
+// fc[32 j]: this lane's slots of the warp's factor cache, (e^{-w ds/4} of block
+// A, of block B) of point x = t + 8 j (filled by the kernel's prologue); fB,
+// cB: whether lane f and lane c are in block B at this step.
 __device__ __forceinline__ long xcol(int c, int t) { return (long)(c >> 2) * 256 + (c & 3) + 4 * t; }
-__device__ __forceinline__ void xtask(bool full, const double2* Zin, double2* Zout, bool fB, bool cB,
-                                      double2* scratch, const double2* fc, int c, int t, const double2* tw,
-                                      const double* tab, double rMd) {
+__device__ __forceinline__ void xtask_full(double2* Z, double2* scratch, int c, int t, const double2* tw,
+                                           const double* tab) {
     double2 v[8];
-    double hf[8], hc[8];
-    const long cx = xcol(c, t);   // x = t in the x-pass layout; + 32 j
+    const long cx = xcol(c, t);
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = Z[cx + 32 * j];
+    line_op(v, t, scratch, 1, tw, ktab(tab, 0, 0));
+#pragma unroll
+    for (int j = 0; j < 8; j++) Z[cx + 32 * j] = v[j];
+    __syncwarp();
+}
+__device__ __forceinline__ void xtask_half(const double2* Zin, double2* Zout, bool fB, bool cB, double2* scratch,
+                                           const double2* fc, int c, int t, const double2* tw, const double* tab,
+                                           double rMd) {
+    double2 v[8];
+    const long cx = xcol(c, t);
 #pragma unroll
     for (int j = 0; j < 8; j++) v[j] = Zin[cx + 32 * j];
-    line_op(v, t, scratch, 1, tw, ktab(tab, full ? 0 : 1, 0));
+    line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
 #pragma unroll
     for (int j = 0; j < 8; j++) {
         const double2 e = fc[32 * j];
-        hf[j] = fB ? e.y : e.x;
-        hc[j] = cB ? e.y : e.x;
+        const double hf = fB ? e.y : e.x, hc = cB ? e.y : e.x;
+        const double qf = (v[j].x * hf) * rMd, qc = (v[j].y * hc) * rMd;
+        v[j] = make_double2(hf * qf, hc * qc);
     }
-    if (full) {
+    __syncwarp();
+    line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
 #pragma unroll
-        for (int j = 0; j < 8; j++)
-            Zout[(long)(t + 8 * j) * P64 + c] =   // u: natural order
-                make_double2((v[j].x * (hf[j] * hf[j])) * rMd, (v[j].y * (hc[j] * hc[j])) * rMd);
-    } else {
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const double qf = (v[j].x * hf[j]) * rMd, qc = (v[j].y * hc[j]) * rMd;
-            v[j] = make_double2(hf[j] * qf, hc[j] * qc);
-        }
-        __syncwarp();
-        line_op(v, t, scratch, 1, tw, ktab(tab, 1, 0));
-#pragma unroll
-        for (int j = 0; j < 8; j++) Zout[cx + 32 * j] = v[j];   // Z3: x-pass layout
-    }
+    for (int j = 0; j < 8; j++) Zout[cx + 32 * j] = v[j];
     __syncwarp();
 }
 
@@ -313,28 +288,29 @@ __device__ __forceinline__ void cluster_sync_all() {
 // product Dx Dy Dz of commuting line operators (exp(-h k^2) is the product of
 // the per-axis factors), so a contour step needs only two grid-wide phases:
 //
-//   x-pass  (4096 columns): Dx of the full step on Z1 -> u; Dx of the first
-//            half step on Z2, the pointwise e^{-w ds/4} work, Dx of the second
-//            half step -> Z3
+//   x-pass  (4096 columns): Dx of the full step on W (in place); Dx of the
+//            first half step on Z2, the pointwise e^{-w ds/4} work, Dx of the
+//            second half step -> Z3
 //   plane   (slab x = s, CTA c of the cluster: columns and rows [32 c, 32 c + 32)):
-//            Dy of the second half step on Z3 (columns) | cluster barrier |
-//            Dz (rows), q[t+1] = (4 qt2 - u) / 3 -> history; the next step's
-//            inputs e^{-w ds/2} q and e^{-w ds/4} q with their Dz (rows) |
-//            cluster barrier | Dy (columns) -> Z1, Z2
+//            Dy of the second half step on Z3 and Dy of the full step on W
+//            (columns) | cluster barrier | Dz of Z3 (rows), u = e^{-w ds/2} W / M,
+//            q[t+1] = (4 qt2 - u) / 3 -> history; the next step's inputs
+//            e^{-w ds/2} q with its Dz -> W, and e^{-w ds/4} q with its Dz
+//            (rows) | cluster barrier | Dy (columns) -> Z2
 //
-// The divisions by M come after the last inverse transform of each operator,
-// where the reference divides.
+// so the full-step field gets Dz at the end of one plane phase, Dx in the
+// x-pass and Dy at the start of the next plane phase (whose first operators
+// have half the lines of its last ones).  The divisions by M come after the
+// last inverse transform of each operator, where the reference divides.
 __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const double* __restrict__ tables) {
     extern __shared__ __align__(128) unsigned char smraw[];
     double2* RA = reinterpret_cast<double2*>(smraw + OFF_RA);
     double2* RB = reinterpret_cast<double2*>(smraw + OFF_RB);
     double* ehA = reinterpret_cast<double*>(smraw + OFF_EHA);
     double* ehB = reinterpret_cast<double*>(smraw + OFF_EHB);
-    double2* su = reinterpret_cast<double2*>(smraw + OFF_U);
     double2* fcache = reinterpret_cast<double2*>(smraw + OFF_FC);
     double2* tw = reinterpret_cast<double2*>(smraw + OFF_TW);
     double* tab = reinterpret_cast<double*>(smraw + OFF_TAB);
-    void* mbar = smraw + OFF_MBAR;
     int* stopped = reinterpret_cast<int*>(smraw + OFF_STOP);
 
     const int b = blockIdx.x;
@@ -343,7 +319,6 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     const double rMd = 1.0 / (double)M64;       // M = 2^18: multiplying by 1/M rounds exactly like dividing
     unsigned* ctr = a.bar;
     unsigned bidx = 0;
-    unsigned mphase = 0;
 
     for (int i = tid; i < 64; i += NT) tw[i] = a.twx[((i & 7) * (i >> 3)) & 63];   // [k1][t]
     for (int i = tid; i < 6 * 64; i += NT) tab[i] = tables[i];
@@ -355,22 +330,18 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
             ehB[(i >> 6) * EHP + (i & 63)] = fb;
         }
     }
-    if (tid == 0) {
-        mbar_init(mbar);
-        *stopped = 0;
-    }
+    if (tid == 0) *stopped = 0;
 
     // x-pass warp index, CTA-fastest so that a phase's tasks spread over all SMs
     const int gwarp = (tid >> 5) * gridDim.x + b;
     const int nwarps = gridDim.x * (NT / 32);
     const int lane = tid & 31, cq = lane >> 3;
     double2* scratch = RB + (tid >> 5) * 256 + cq * 64;
-    double2* fc = fcache + (tid >> 5) * 256 + lane;   // this lane's x-pass factors (warps < XW)
-    double2* ug = reinterpret_cast<double2*>(a.uf);   // interleaved (u_f, u_c)
-    // the factors (e^{-w ds/4} of A, of B) of the warp's x-pass task, x = t + 8 j
-    // of its column, for the whole sweep (the task is the same every step)
-    if (gwarp < 2 * (P64 / 4) && (tid >> 5) < XW) {
-        const int column = (gwarp >= P64 / 4 ? gwarp - P64 / 4 : gwarp) * 4 + cq;
+    double2* fc = fcache + (tid >> 5) * 256 + lane;   // this lane's x-pass factors (warps < XH)
+    // the factors (e^{-w ds/4} of A, of B) of the warp's half-step x-pass task,
+    // x = t + 8 j of its column, for the whole sweep (the task is the same every step)
+    if (gwarp < P64 / 4 && (tid >> 5) < XH) {
+        const int column = gwarp * 4 + cq;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const long i = (long)(t + 8 * j) * P64 + column;
@@ -386,73 +357,87 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     auto gsync = [&]() { grid_sync(ctr, a.err, ++bidx, stopped); };
 
     // The next step's inputs from q[st] (rows, held by the threads of field 0:
-    // row r, z = t + 8 j): e^{-w ds/2} q (field 0) and e^{-w ds/4} q (field 1),
-    // Dz on the rows, cluster barrier, Dy on the columns -> Z1, Z2
+    // row r, z = t + 8 j): e^{-w ds/2} q (field 0) gets Dz and goes to W (its Dx
+    // and Dy follow); e^{-w ds/4} q (field 1) gets Dz, and after a cluster
+    // barrier Dy on the columns -> Z2
     auto next_inputs = [&](double2 (&v)[8], int st) {
         const PlaneIx ix = plane_ix();
         const int c = ix.c, r = ix.r, f = ix.f, ze0 = ix.ze0;
+        const int slab = (int)(ix.soff >> 12);
         const double* nf = sh_f(st);
         const double* nc = sh_c(st);
-        double2* Q1 = RA + 32 * QP;
+        double2* row = RA + (f * 32 + r) * QP;   // field f's row r: Dz exchange area (field 1: and result)
+        if (f == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; j++) row[32 * QP + t + 8 * j] = v[j];   // q for field 1
+        }
+        __syncthreads();
         if (f == 0) {
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                Q1[r * QP + t + 8 * j] = v[j];
                 const double gf = nf[ze0 + 8 * j], gc = nc[ze0 + 8 * j];
                 v[j] = make_double2((gf * gf) * v[j].x, (gc * gc) * v[j].y);
             }
-        }
-        __syncthreads();
-        if (f == 1) {
+            line_op(v, t, row, 1, tw, ktab(tab, 0, 2));
+            // row y = 32 c + r, z = t + 8 j in the x-pass layout
+            double2* W = a.Z1 + xq(slab, 32 * c + r, t);
+#pragma unroll
+            for (int j = 0; j < 8; j++) W[512 * j] = v[j];
+        } else {
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const double2 q = Q1[r * QP + t + 8 * j];
+                const double2 q = row[t + 8 * j];
                 v[j] = make_double2(nf[ze0 + 8 * j] * q.x, nc[ze0 + 8 * j] * q.y);
             }
-        }
-        double2* row = RA + (f * 32 + r) * QP;
-        line_op(v, t, row, 1, tw, ktab(tab, f, 2));
-        __syncwarp();
+            line_op(v, t, row, 1, tw, ktab(tab, 1, 2));
+            __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 8; j++) row[t + 8 * j] = v[j];
+            for (int j = 0; j < 8; j++) row[t + 8 * j] = v[j];
+        }
         cluster_sync_all();
-        // column z = 32 c + r of field f; element y = t + 8 j is row t + 8 (j & 3) of CTA j / 4
-        {
-            // RA of CTA 0 (rows [0, 32)) and of CTA 1 ([32, 64))
-            const double2* p = RA + f * 32 * QP + 32 * c + r + t * QP;
-            const unsigned lo = cluster_addr(p, 0), hi = cluster_addr(p, 1);
+        if (f == 1) {
+            // column z = 32 c + r; element y = t + 8 j is row t + 8 (j & 3) of CTA j / 4
+            {
+                const double2* p = RA + 32 * QP + 32 * c + r + t * QP;
+                const unsigned lo = cluster_addr(p, 0), hi = cluster_addr(p, 1);
 #pragma unroll
-            for (int j = 0; j < 8; j++) v[j] = ld_cluster((j < 4 ? lo : hi) + 16 * 8 * QP * (j & 3));
+                for (int j = 0; j < 8; j++) v[j] = ld_cluster((j < 4 ? lo : hi) + 16 * 8 * QP * (j & 3));
+            }
+            line_op(v, t, RB + r, SP, tw, ktab(tab, 1, 1));
+            double2* Zg = a.Z2 + xq(slab, t, 32 * c + r);
+#pragma unroll
+            for (int j = 0; j < 8; j++) Zg[8 * j * 16 * 256] = v[j];   // y = t + 8 j
         }
-        line_op(v, t, RB + f * 32 + r, SP, tw, ktab(tab, f, 1));
-        double2* Zg = (f == 0 ? a.Z1 : a.Z2) + xq((int)(ix.soff >> 12), t, 32 * c + r);
-#pragma unroll
-        for (int j = 0; j < 8; j++) Zg[8 * j * 16 * 256] = v[j];   // y = t + 8 j
     };
 
     // Step st = -1 forms the first inputs from the chain heads; every later
     // step is an x-pass and a plane phase.
     for (int st = -1; st < a.Ns; st++) {
         if (st >= 0) {
-            // ---- x-pass: Z1 -> u, Z2 -> Z3 (the longer Z2 tasks first) --------
+            // ---- x-pass: W in place, Z2 -> Z3 (the longer Z2 tasks first) -----
             for (int task = gwarp; task < 2 * (P64 / 4); task += nwarps) {
-                // one task a warp, by warps < XW (the launcher's grid ensures it)
-                if ((tid >> 5) >= XW || task + nwarps < 2 * (P64 / 4)) { atomicExch(a.err, 4); break; }
-                const bool full = task >= P64 / 4;
-                const int column = (full ? task - P64 / 4 : task) * 4 + cq;
-                xtask(full, full ? a.Z1 : a.Z2, full ? ug : a.Z3, st >= a.LA, st < a.LB, scratch, fc, column, t, tw,
-                      tab, rMd);
+                // one task a warp; the half-step tasks on warps < XH (the
+                // launcher's grid ensures both)
+                if ((tid >> 5) >= XW || task + nwarps < 2 * (P64 / 4) || (task < P64 / 4 && (tid >> 5) >= XH)) {
+                    atomicExch(a.err, 4);
+                    break;
+                }
+                if (task < P64 / 4)
+                    xtask_half(a.Z2, a.Z3, st >= a.LA, st < a.LB, scratch, fc, task * 4 + cq, t, tw, tab, rMd);
+                else
+                    xtask_full(a.Z1, scratch, (task - P64 / 4) * 4 + cq, t, tw, tab);
             }
             gsync();
         }
 
-        // ---- plane: Z3 -> q[st+1] -> next Z1 / Z2 ------------------------------
+        // ---- plane: Z3, W -> q[st+1] -> next W, Z2 -----------------------------
         const bool next = st + 1 < a.Ns;
         if (planar) {
             double2 v[8];
             const PlaneIx ix = plane_ix();
             const int c = ix.c, r = ix.r, f = ix.f, ze0 = ix.ze0;
-            const long soff = ix.soff, hoff = ix.hoff;
+            const int slab = (int)(ix.soff >> 12);
+            const long hoff = ix.hoff;
             if (st < 0) {
                 if (f == 0) {
 #pragma unroll
@@ -463,53 +448,55 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                 }
             } else {
                 if (f == 0) {
-                    // Dy of column z = 32 c + r (y = t + 8 j)
-                    const double2* Z3 = a.Z3 + xq((int)(soff >> 12), t, 32 * c + r);
+                    // Dy (second half step) of Z3's column z = 32 c + r (y = t + 8 j)
+                    const double2* Z3 = a.Z3 + xq(slab, t, 32 * c + r);
 #pragma unroll
-                    for (int j = 0; j < 8; j++) v[j] = Z3[8 * j * 16 * 256];   // y = t + 8 j
+                    for (int j = 0; j < 8; j++) v[j] = Z3[8 * j * 16 * 256];
                     double2* col = RB + r;
                     line_op(v, t, col, PB, tw, ktab(tab, 1, 1));
-                    if (tid == 0) {
-                        // this CTA's rows of u, by a bulk copy once the Z3 loads are
-                        // done (they share L2 bandwidth; u is needed after Dz).  The
-                        // proxy fence orders earlier generic-proxy accesses (other
-                        // CTAs' u stores, this CTA's reads of su) before the copy.
-                        asm volatile("fence.proxy.async;" ::: "memory");
-                        bulk_load(su, ug + hoff, H64 * 16, mbar);
-                    }
                     __syncwarp();
 #pragma unroll
                     for (int j = 0; j < 8; j++) col[(t + 8 * j) * PB] = v[j];
+                } else {
+                    // Dy (full step) of W's column z = 32 c + r, stored with row y
+                    // at RB[UC + 32 y + (r ^ (y & 7))] (conflict-free both ways)
+                    const double2* W = a.Z1 + xq(slab, t, 32 * c + r);
+#pragma unroll
+                    for (int j = 0; j < 8; j++) v[j] = W[8 * j * 16 * 256];
+                    line_op(v, t, RA + (32 + r) * QP, 1, tw, ktab(tab, 0, 1));
+#pragma unroll
+                    for (int j = 0; j < 8; j++) RB[UC + (t + 8 * j) * 32 + (r ^ t)] = v[j];
                 }
                 cluster_sync_all();
                 if (f == 0) {
                     // Dz of row y = 32 c + r; element z = t + 8 j is column t + 8 (j & 3) of CTA j / 4
                     {
-                        // RB of CTA 0 (columns [0, 32)) and of CTA 1 ([32, 64))
                         const double2* p = RB + (32 * c + r) * PB + t;
                         const unsigned lo = cluster_addr(p, 0), hi = cluster_addr(p, 1);
 #pragma unroll
                         for (int j = 0; j < 8; j++) v[j] = ld_cluster((j < 4 ? lo : hi) + 16 * 8 * (j & 3));
                     }
                     line_op(v, t, RA + r * QP, 1, tw, ktab(tab, 1, 2));
-                    if (!mbar_wait(mbar, mphase)) atomicExch(a.err, 3);
                     const double* ef = sh_f(st);
                     const double* ec = sh_c(st);
                     double* of = a.hf + (long)(st + 1) * M64 + hoff + r * 64 + t;
                     double* oc = a.hc + (long)(st + 1) * M64 + hoff + r * 64 + t;
+                    // W of row y: column z = t + 8 j sits at column (t ^ (y & 7)) + 8 (j & 3) of CTA j / 4
+                    const double2* pu = RB + UC + (32 * c + r) * 32 + (t ^ (r & 7));
+                    const unsigned ulo = cluster_addr(pu, 0), uhi = cluster_addr(pu, 1);
 #pragma unroll
                     for (int j = 0; j < 8; j++) {
                         const double hf = ef[ze0 + 8 * j], hc = ec[ze0 + 8 * j];
-                        const double2 u = su[r * 64 + t + 8 * j];
+                        const double2 w = ld_cluster((j < 4 ? ulo : uhi) + 16 * 8 * (j & 3));
+                        const double uf = (w.x * (hf * hf)) * rMd, uc = (w.y * (hc * hc)) * rMd;
                         double qf = (v[j].x * hf) * rMd, qc = (v[j].y * hc) * rMd;
-                        qf = div_rn(4.0 * qf - u.x, 3.0, 1.0 / 3.0);
-                        qc = div_rn(4.0 * qc - u.y, 3.0, 1.0 / 3.0);
+                        qf = div_rn(4.0 * qf - uf, 3.0, 1.0 / 3.0);
+                        qc = div_rn(4.0 * qc - uc, 3.0, 1.0 / 3.0);
                         of[8 * j] = qf;
                         oc[8 * j] = qc;
                         v[j] = make_double2(qf, qc);
                     }
                 }
-                mphase ^= 1u;
             }
             if (next) next_inputs(v, st + 1);
         }
@@ -553,10 +540,10 @@ int sweep64_prepare() {
     int nclusters = 0;
     PS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, sweep64_kernel, &cfg));
     nclusters = std::min(nclusters, sms / 2);
-    // 64 clusters own the slabs; every x-pass warp with a task keeps its
-    // factors resident, so the 2048 tasks need one warp each among the first
-    // XW warps of every CTA
-    if (nclusters < 64 || 2 * nclusters * XW < 2 * (P64 / 4)) return 0;
+    // 64 clusters own the slabs; every x-pass warp with a half-step task keeps
+    // its factors resident, so the 2048 tasks need one warp each among the
+    // first XW warps of every CTA, the 1024 half-step tasks among the first XH
+    if (nclusters < 64 || 2 * nclusters * XW < 2 * (P64 / 4) || 2 * nclusters * XH < P64 / 4) return 0;
     char line[160];
     std::snprintf(line, sizeof(line), "64^3 sweep: %d clusters of 2 CTAs resident, grid %d\n", nclusters,
                   2 * nclusters);

@@ -126,8 +126,11 @@ def test_c2_trajectory_parity_and_where_it_diverges(ps):
       way the GPU and the oracle (two FFT orders) leave each other.  Along the
       whole recorded trajectory (fixture c2, up to the workload's 1000
       iterations) the GPU-oracle difference of H stays within 100 times that
-      perturbation's spread (floor 1e-12).  The first iteration where H leaves
-      1e-10 is printed."""
+      perturbation's spread (floor 1e-12), the spread at iteration k being the
+      largest perturbed-run difference within 10 iterations of k (the
+      difference of two such runs changes sign now and then, so its value at
+      a single iteration can be arbitrarily small).  The first iteration where
+      H leaves 1e-10 is printed."""
     from polystring_b200 import workloads
     fx, fs = _trajectory_fixture("c2"), _trajectory_fixture("c2_start")
     cfg = workloads.config("C2")
@@ -150,7 +153,11 @@ def test_c2_trajectory_parity_and_where_it_diverges(ps):
             if j == 0:
                 assert d < 1e-10, ((j + 1) * every, f, d)
             assert d <= 100.0 * max(dp, 1e-12), ((j + 1) * every, f, d, dp)
-    assert np.all(e_or <= 100.0 * np.maximum(e_pt, 1e-12)), int(np.argmax(e_or / np.maximum(e_pt, 1e-12))) + 1
+    win = 10
+    spread = np.array([e_pt[max(0, k - win):k + win + 1].max() for k in range(n)])
+    ratio = e_or / np.maximum(spread, 1e-12)
+    k = int(np.argmax(ratio))
+    assert ratio[k] <= 100.0, (k + 1, e_or[k], spread[k])
     over = np.nonzero(e_or > 1e-10)[0]
     print("C2 trajectory: H/Q within 1e-10 of the oracle through iteration %d of %d; at 100: oracle %.1e, "
           "1e-15 perturbation %.1e" % (over[0] if len(over) else n, n, e_or[min(99, n - 1)], e_pt[min(99, n - 1)]))
