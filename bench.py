@@ -322,6 +322,7 @@ def uneven_batch(ps, n=256, iters=2):
     tb = b.update_timed(iters) / 1e3
     work = b.gridpoint_steps() * iters
     launches = b.launches_per_iteration()
+    launches_prop = b.launches_per_propagate()
     del b
     ts = ts_abc = 0.0
     for sp in specs:
@@ -344,6 +345,10 @@ def uneven_batch(ps, n=256, iters=2):
                       "%d of 300 iterations timed" % (n, n_ab, n_abc, sizes, iters),
             "batch_gridpt_steps_per_s": work / tb, "sequential_gridpt_steps_per_s": work / (ts + ts_abc),
             "speedup_vs_sequential": (ts + ts_abc) / tb, "launches_per_batch_iteration": launches,
+            "launches_split": {"propagators": launches_prop, "q_density_field_update": launches - launches_prop,
+                               "note": "one persistent sweep launch covers all contour steps of the solves it "
+                                       "carries; the rest are each member's own small Q, density and Anderson "
+                                       "kernels, replayed in the same graph"},
             "sequential_s": {"ab": ts, "abc": ts_abc},
             "timing": "CUDA events on the batch stream and each AB solve's stream; host clock around "
                       "synchronised runs for each ABC solve"}

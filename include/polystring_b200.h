@@ -341,6 +341,9 @@ int ps_batch_ab_residual(ps_batch_ab* b, int k, double* res);
 int ps_batch_ab_get(ps_batch_ab* b, int k, int which, double* out);
 int ps_batch_ab_synchronize(ps_batch_ab* b);
 int ps_batch_ab_launches_per_iteration(ps_batch_ab* b);
+/* of them, the propagator launches (persistent sweeps and grouped line passes);
+   the rest are the members' Q, density and field-update kernels */
+int ps_batch_ab_launches_per_propagate(ps_batch_ab* b);
 /* sum over solves of 2 Ns M: gridpoint contour steps of one batch iteration */
 int ps_batch_ab_gridpoint_steps(ps_batch_ab* b, double* out);
 

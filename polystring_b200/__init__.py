@@ -485,6 +485,11 @@ class BatchAB:
     def launches_per_iteration(self):
         return lib().ps_batch_ab_launches_per_iteration(self._h)
 
+    def launches_per_propagate(self):
+        """Propagator launches of one batch iteration (the rest are the
+        members' Q, density and field-update kernels)."""
+        return lib().ps_batch_ab_launches_per_propagate(self._h)
+
     def gridpoint_steps(self):
         v = ctypes.c_double()
         capi.check(lib().ps_batch_ab_gridpoint_steps(self._h, ctypes.byref(v)))

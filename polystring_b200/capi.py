@@ -137,6 +137,7 @@ SIGNATURES = [
     ("ps_batch_ab_get", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _dp]),
     ("ps_batch_ab_synchronize", ctypes.c_int, [_vp]),
     ("ps_batch_ab_launches_per_iteration", ctypes.c_int, [_vp]),
+    ("ps_batch_ab_launches_per_propagate", ctypes.c_int, [_vp]),
     ("ps_batch_ab_gridpoint_steps", ctypes.c_int, [_vp, _dp]),
 ]
 

@@ -290,6 +290,7 @@ void BatchAB::enqueue_iteration() {
             pass(K_END);
         }
     }
+    launches_prop_ = launches;
     for (auto* m : m_) {
         m->enqueue_post(st_);
         launches += m->launches_per_iteration() - m->launches_per_propagate();

@@ -25,6 +25,7 @@ public:
     double update_timed(int n);
     void sync();
     int launches_per_iteration() const { return launches_; }
+    int launches_per_propagate() const { return launches_prop_; }
     // sum over solves of 2 Ns M: gridpoint contour steps of one iteration
     double gridpoint_steps_per_iteration() const;
 
@@ -60,7 +61,7 @@ private:
     std::vector<int> own_;                   // solves propagated by their own 64^3 sweep
     cudaStream_t st_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
-    int launches_ = 0;
+    int launches_ = 0, launches_prop_ = 0;
 };
 
 }  // namespace ps

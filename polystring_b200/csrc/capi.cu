@@ -560,6 +560,8 @@ int ps_batch_ab_synchronize(ps_batch_ab* b) {
 
 int ps_batch_ab_launches_per_iteration(ps_batch_ab* b) { return b ? b->ctx->launches_per_iteration() : -1; }
 
+int ps_batch_ab_launches_per_propagate(ps_batch_ab* b) { return b ? b->ctx->launches_per_propagate() : -1; }
+
 int ps_batch_ab_gridpoint_steps(ps_batch_ab* b, double* out) {
     return guarded([&] {
         if (!b || !out) throw Error(PS_ERR_INVALID, "null argument");
