@@ -32,8 +32,6 @@
 // e^{-w ds/2} is formed as (e^{-w ds/4})^2, and the k-space factors as
 // per-axis tables; both agree with the reference's direct exp() evaluations
 // to a few ulps.
-#include <cooperative_groups.h>
-
 #include <algorithm>
 #include <cstdio>
 
@@ -41,8 +39,6 @@
 #include "fft_core.cuh"
 #include "engine.h"
 #include "sweep.h"
-
-namespace cg = cooperative_groups;
 
 namespace ps {
 
@@ -55,9 +51,9 @@ constexpr int NT = 512;
 constexpr long long kSpin = 20000000;
 
 // shared memory map (bytes)
-//   RA: rows of pitch QP: Dz exchange areas of both fields (rows 0-31 the
-//       full-step field, 32-63 the half-step one), the half-step input after
-//       Dz, read by both CTAs for Dy; Dy exchange areas of the full-step field
+//   RA: 64 rows of pitch QP: rows 0-31 the Dz exchange areas of Z3 and of the
+//       full-step input; rows 32-63 the Dy exchange areas of W's columns, then
+//       q and the half-step input, whose rows after Dz both CTAs read for Dy
 //   RB: Z3 after Dy, the CTA's 32 columns (64 rows of pitch PB), and behind
 //       it the full-step result after Dy, the CTA's 32 columns (64 rows of 32,
 //       swizzled), both read by both CTAs for the rows; the Dy exchange areas
