@@ -17,9 +17,9 @@
 // solves of one shape share one cooperative launch for all their contour
 // steps (sweep.cu, a descriptor per solve, the CTAs split between solves),
 // 64^3 solves run their own 64^3 sweep (sweep64.cu), which fills the GPU
-// alone.  One batch iteration -- all propagators, then every member's Q,
-// densities and field update -- is captured once as a CUDA graph and
-// replayed.
+// alone (and so do 64^3 triblocks).  One batch iteration -- all propagators,
+// then every member's Q, densities and field update -- is captured once as a
+// CUDA graph and replayed.
 #include "batch_ab.h"
 
 #include <algorithm>
@@ -70,9 +70,13 @@ BatchAB::BatchAB(const std::vector<ModelABParams>& ps, const std::vector<ModelAB
             else if (m_[k]->persistent_sweep()) swept.push_back(k);
             else passes.push_back(k);
         }
-        // triblocks likewise (their grids' generic sweep, else grouped line passes)
-        for (int j = 0; j < (int)t_.size(); j++)
-            (t_[j]->persistent_sweep() ? swept : passes).push_back((int)m_.size() + j);
+        // triblocks likewise (their own 64^3 sweep, their grids' generic sweep,
+        // else grouped line passes)
+        for (int j = 0; j < (int)t_.size(); j++) {
+            const int k = (int)m_.size() + j;
+            if (t_[j]->persistent_sweep64()) own_.push_back(k);
+            else (t_[j]->persistent_sweep() ? swept : passes).push_back(k);
+        }
         build_sweeps(swept);
         // groups: same number of long axes (the step's pass sequence) and the
         // same schedule on each axis role (one kernel per grouped pass)
@@ -262,7 +266,8 @@ void BatchAB::enqueue_iteration() {
         launches++;
     }
     for (int k : own_) {
-        m_[k]->enqueue_propagate(st_);
+        if (k < (int)m_.size()) m_[k]->enqueue_propagate(st_);
+        else t_[k - (int)m_.size()]->enqueue_propagate(st_);
         launches++;
     }
     int Ns_max = 0;

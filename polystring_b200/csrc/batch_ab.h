@@ -58,7 +58,7 @@ private:
     std::vector<ModelABC*> t_;
     std::vector<Group> groups_;
     std::vector<SweepChunk> chunks_;
-    std::vector<int> own_;                   // solves propagated by their own 64^3 sweep
+    std::vector<int> own_;                   // solves propagated by their own 64^3 sweep (AB and ABC indices)
     cudaStream_t st_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     int launches_ = 0, launches_prop_ = 0;

@@ -434,19 +434,7 @@ ModelAB::ModelAB(const ModelABParams& p, bool batch_member) : p_(p) {
     use_sweep_ = allow && p.mde == 0 && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
     if (use_sweep64_) {
         swZ_.alloc(6 * (size_t)M_);
-        // per-axis factors exp(h cc_axis r^2), h = ds (full) and ds/2 (half)
-        const double PI = 3.14159265358979323846;
-        std::vector<double> tab(6 * 64);
-        const int Ls[3] = {p.Lx, p.Ly, p.Lz};
-        for (int half = 0; half < 2; half++)
-            for (int ax = 0; ax < 3; ax++) {
-                double cc = -4.0 * PI * PI / (p_.cell.l[ax] * p_.cell.l[ax]);
-                double h = half ? 0.5 * dsA_ : dsA_;
-                for (int i = 0; i < 64; i++) {
-                    int ri = (i < Ls[ax] / 2 + 1) ? i : Ls[ax] - i;
-                    tab[half * 192 + ax * 64 + i] = exp(h * (cc * ri * ri));
-                }
-            }
+        const std::vector<double> tab = sweep64_axis_tables(p_.cell.l, dsA_);
         swTab_.alloc(tab.size());
         PS_CUDA(cudaMemcpy(swTab_.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
         PS_CUDA(cudaMalloc(&swbar_, 64 * sizeof(unsigned)));

@@ -292,8 +292,11 @@ public:
     void enqueue_propagate(cudaStream_t s);
     void enqueue_post(cudaStream_t s);
     int launches_post() const { return 2 + 3 + (p_.scft == 1 ? 4 : 1); }
-    // the generic persistent sweep (32^3, 48^3, 64^3 grids) with three factor sets
+    // the generic persistent sweep (32^3, 48^3 grids; 64^3 where the 64^3
+    // sweep cannot run) with three factor sets
     bool persistent_sweep() const { return use_sweep_; }
+    // the 64^3 sweep (sweep64.cu) with three factor sets
+    bool persistent_sweep64() const { return use_sweep64_; }
     SweepArgs sweep_descriptor() const;
     const ModelABCParams& params() const { return p_; }
 
@@ -312,8 +315,9 @@ private:
     long iter_ = 0;
     bool fields_set_ = false;
     bool use_sweep_ = false;
+    bool use_sweep64_ = false;
     int sweep_grid_ = 0;
-    DevBuf swZ_, swU_, swL1_, swL2_;
+    DevBuf swZ_, swU_, swL1_, swL2_, swTab_;
     unsigned* swbar_ = nullptr;
     int* swerr_ = nullptr;
 };

@@ -21,9 +21,10 @@
 //     coefficient set from U = UA + UB + UC, V = VA + VB + VC;
 //   * Hw = mean(chiAB phiA phiB + chiBC phiB phiC + chiAC phiA phiC -
 //     sum_X wX phiX), Hs = -ln Q; the residuals of Model_AB with a third field.
-// Incompressible, RQM4, orthogonal k^2 table.  Propagation: the generic
-// persistent sweep (sweep.cu) on 32^3, 48^3 and 64^3 grids, given three
-// factor sets; the packed line passes (PairChain) on other grids.
+// Incompressible, RQM4, orthogonal k^2 table.  Propagation: the 64^3 sweep
+// (sweep64.cu) on 64^3 grids and the generic persistent sweep (sweep.cu) on
+// 32^3 and 48^3 grids, each given three factor sets; the packed line passes
+// (PairChain) on other grids.
 #include <cmath>
 #include <cstdlib>
 #include <string>
@@ -65,7 +66,24 @@ ModelABC::ModelABC(const ModelABCParams& p) : p_(p) {
     }
     chain_->set_tables(L1, L2);
     const char* force = getenv("PS_B200_LINE_PASSES");
-    use_sweep_ = !(force && force[0] == '1') && sweep_supported(p.Lx, p.Ly, p.Lz);
+    const char* generic = getenv("PS_B200_GENERIC_SWEEP");
+    const bool allow = !(force && force[0] == '1');
+    // 64^3 grids take the 64^3 sweep where its clusters fit (as Model_AB)
+    use_sweep64_ = allow && sweep64_supported(p.Lx, p.Ly, p.Lz) && !(generic && generic[0] == '1');
+    if (use_sweep64_) {
+        sweep_grid_ = sweep64_prepare();
+        use_sweep64_ = sweep_grid_ > 0;
+    }
+    use_sweep_ = allow && !use_sweep64_ && sweep_supported(p.Lx, p.Ly, p.Lz);
+    if (use_sweep64_) {
+        swZ_.alloc(6 * (size_t)M_);
+        const std::vector<double> tab = sweep64_axis_tables(p_.cell.l, ds_[0]);
+        swTab_.alloc(tab.size());
+        PS_CUDA(cudaMemcpy(swTab_.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+        PS_CUDA(cudaMalloc(&swbar_, 64 * sizeof(unsigned)));
+        PS_CUDA(cudaMalloc(&swerr_, sizeof(int)));
+        PS_CUDA(cudaMemset(swerr_, 0, sizeof(int)));
+    }
     if (use_sweep_) {
         sweep_grid_ = sweep_prepare(p.Lx, p.Ly, p.Lz);
         swZ_.alloc(6 * (size_t)M_);
@@ -98,7 +116,7 @@ ModelABC::ModelABC(const ModelABCParams& p) : p_(p) {
     launch_fill(hf_.p, M_, 1.0, st_);
     launch_fill(hc_.p, M_, 1.0, st_);
     launch_fill(yita_.p, M_, 0.0, st_);
-    if (!use_sweep_) chain_->autotune(st_);
+    if (!use_sweep_ && !use_sweep64_) chain_->autotune(st_);
     PS_CUDA(cudaStreamSynchronize(st_));
 }
 
@@ -153,6 +171,17 @@ SweepArgs ModelABC::sweep_descriptor() const {
 }
 
 void ModelABC::enqueue_propagate(cudaStream_t s) {
+    if (use_sweep64_) {
+        SweepArgs a{};
+        a.hf = hf_.p; a.hc = hc_.p;
+        a.Z1 = swZ_.c(); a.Z2 = swZ_.c() + M_; a.Z3 = swZ_.c() + 2 * M_;
+        a.eFA = eF_[0].p; a.eHA = eH_[0].p; a.eFB = eF_[1].p; a.eHB = eH_[1].p; a.eFC = eF_[2].p; a.eHC = eH_[2].p;
+        a.LA = L_[0]; a.LB = L_[1]; a.LC = L_[2]; a.Ns = Ns_;
+        a.bar = swbar_; a.err = swerr_;
+        PS_CUDA(cudaMemsetAsync(swbar_, 0, 64 * sizeof(unsigned), s));
+        sweep64_launch(a, swTab_.p, sweep_grid_, s);
+        return;
+    }
     if (use_sweep_) {
         const SweepArgs a = sweep_descriptor();
         PS_CUDA(cudaMemsetAsync(swbar_, 0, 32 * sizeof(unsigned), s));

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace ps {
 
 struct SweepArgs {
@@ -33,6 +35,9 @@ bool sweep64_supported(int Lx, int Ly, int Lz);
 // sets kernel attributes, builds twiddles; returns the grid (two-CTA clusters,
 // one CTA per SM), or 0 when too few clusters can be resident on this device
 int sweep64_prepare();
+// the sweep's per-axis k-space factors exp(h cc_axis r^2) of a 64^3 grid on an
+// orthogonal cell of lengths l, h = ds (full step) then ds / 2: 6 x 64 doubles
+std::vector<double> sweep64_axis_tables(const double l[3], double ds);
 void sweep64_launch(const SweepArgs& a, const double* tables, int grid, cudaStream_t st);
 // sets kernel attributes, builds twiddles; returns the cooperative grid size
 int sweep_prepare(int Lx, int Ly, int Lz);

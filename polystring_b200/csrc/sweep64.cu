@@ -33,6 +33,7 @@
 // per-axis tables; both agree with the reference's direct exp() evaluations
 // to a few ulps.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "ps_internal.h"
@@ -58,8 +59,12 @@ constexpr long long kSpin = 20000000;
 //       it the full-step result after Dy, the CTA's 32 columns (64 rows of 32,
 //       swizzled), both read by both CTAs for the rows; the Dy exchange areas
 //       of the half-step input (32 lines, slot pitch SP); x-pass exchange areas
-//   FC: the factors of the four columns of each warp with a half-step x-pass
-//       task, for the whole sweep (a warp's task is the same every step)
+//   EH: the CTA's 32 rows of e^{-w ds/4} of each block (A, B and, for a
+//       linear ABC triblock, C), for the whole sweep
+//   FC: the factor pair (lane f's block, lane c's block) of the four columns
+//       of each warp with a half-step x-pass task; a warp's task is the same
+//       every step, so the pairs are loaded again only when a lane changes
+//       block
 constexpr int QP = 65;                                         // complex
 constexpr int PB = 33;
 constexpr int SP = 65;
@@ -81,10 +86,14 @@ constexpr int OFF_TW = OFF_FC + XH * 256 * 16;                 // 64 double2
 constexpr int OFF_TAB = OFF_TW + 64 * 16;                      // 6 x 64 double: x,y,z tables for L1 then L2
 constexpr int OFF_STOP = OFF_TAB + 6 * 64 * 8;                 // grid barriers no longer waited (int)
 constexpr int SMEM64 = OFF_STOP + 16;
+// block C's rows, at the end: only the launches of linear ABC triblocks ask
+// for the extra shared memory (the diblocks' launches keep it as L1 cache)
+constexpr int OFF_EHC = SMEM64;
+constexpr int SMEM64_ABC = OFF_EHC + 32 * EHP * 8;
 static_assert((UC + H64) * 16 <= SZ_RB, "Z3 and full-step columns fit in RB");
 static_assert(16 * 256 * 16 <= SZ_RB && (31 + 63 * SP + 1) * 16 <= SZ_RB, "exchange areas fit in RB");
 static_assert(OFF_FC % 16 == 0 && OFF_STOP % 8 == 0, "alignment");
-static_assert(SMEM64 <= 232448, "shared memory of one CTA");
+static_assert(SMEM64_ABC <= 232448, "shared memory of one CTA");
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -195,9 +204,11 @@ __device__ __forceinline__ long xq(int x, int y, int z) { return ((long)((y << 4
 //               factor e^{-w ds/2} / M follow in the plane phase)
 //   half step (Z2 -> Z3): Dx of the half step, qt = e^{-w ds/4} v / M, the
 //               second half step's input e^{-w ds/4} qt and its Dx
-// fc[32 j]: this lane's slots of the warp's factor cache, (e^{-w ds/4} of block
-// A, of block B) of point x = t + 8 j (filled by the kernel's prologue); fB,
-// cB: whether lane f and lane c are in block B at this step.
+// fc[32 j]: this lane's slots of the warp's factor cache, a pair of e^{-w ds/4}
+// at point x = t + 8 j: for a diblock (block A, block B) for the whole sweep,
+// fB and cB telling whether lane f and lane c are in block B at this step; for
+// a triblock (lane f's block, lane c's block), loaded again by xfill when a
+// lane changes block, fB = false and cB = true.
 __device__ __forceinline__ long xcol(int c, int t) { return (long)(c >> 2) * 256 + (c & 3) + 4 * t; }
 __device__ __forceinline__ void xtask_full(double2* Z, double2* scratch, int c, int t, const double2* tw,
                                            const double* tab) {
@@ -209,6 +220,13 @@ __device__ __forceinline__ void xtask_full(double2* Z, double2* scratch, int c, 
 #pragma unroll
     for (int j = 0; j < 8; j++) Z[cx + 32 * j] = v[j];
     __syncwarp();
+}
+__device__ __forceinline__ void xfill(const double* ef, const double* ec, double2* fc, int c, int t) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const long i = (long)(t + 8 * j) * P64 + c;   // natural order
+        fc[32 * j] = make_double2(ef[i], ec[i]);
+    }
 }
 __device__ __forceinline__ void xtask_half(const double2* Zin, double2* Zout, bool fB, bool cB, double2* scratch,
                                            const double2* fc, int c, int t, const double2* tw, const double* tab,
@@ -298,12 +316,14 @@ __device__ __forceinline__ void cluster_sync_all() {
 // x-pass and Dy at the start of the next plane phase (whose first operators
 // have half the lines of its last ones).  The divisions by M come after the
 // last inverse transform of each operator, where the reference divides.
+template <bool TRI>   // TRI: a linear ABC triblock (three factor sets)
 __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const double* __restrict__ tables) {
     extern __shared__ __align__(128) unsigned char smraw[];
     double2* RA = reinterpret_cast<double2*>(smraw + OFF_RA);
     double2* RB = reinterpret_cast<double2*>(smraw + OFF_RB);
     double* ehA = reinterpret_cast<double*>(smraw + OFF_EHA);
     double* ehB = reinterpret_cast<double*>(smraw + OFF_EHB);
+    double* ehC = reinterpret_cast<double*>(smraw + OFF_EHC);
     double2* fcache = reinterpret_cast<double2*>(smraw + OFF_FC);
     double2* tw = reinterpret_cast<double2*>(smraw + OFF_TW);
     double* tab = reinterpret_cast<double*>(smraw + OFF_TAB);
@@ -321,9 +341,9 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     if (planar) {
         const long hoff = plane_ix().hoff;
         for (int i = tid; i < H64; i += NT) {
-            const double fa = a.eHA[hoff + i], fb = a.eHB[hoff + i];
-            ehA[(i >> 6) * EHP + (i & 63)] = fa;
-            ehB[(i >> 6) * EHP + (i & 63)] = fb;
+            ehA[(i >> 6) * EHP + (i & 63)] = a.eHA[hoff + i];
+            ehB[(i >> 6) * EHP + (i & 63)] = a.eHB[hoff + i];
+            if constexpr (TRI) ehC[(i >> 6) * EHP + (i & 63)] = a.eHC[hoff + i];
         }
     }
     if (tid == 0) *stopped = 0;
@@ -334,21 +354,37 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
     const int lane = tid & 31, cq = lane >> 3;
     double2* scratch = RB + (tid >> 5) * 256 + cq * 64;
     double2* fc = fcache + (tid >> 5) * 256 + lane;   // this lane's x-pass factors (warps < XH)
-    // the factors (e^{-w ds/4} of A, of B) of the warp's half-step x-pass task,
-    // x = t + 8 j of its column, for the whole sweep (the task is the same every step)
-    if (gwarp < P64 / 4 && (tid >> 5) < XH) {
-        const int column = gwarp * 4 + cq;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const long i = (long)(t + 8 * j) * P64 + column;
-            fc[32 * j] = make_double2(a.eHA[i], a.eHB[i]);
-        }
+    if constexpr (!TRI) {
+        // a diblock's (A, B) factor pairs of the warp's half-step x-pass task, x =
+        // t + 8 j of its column, for the whole sweep (the task is the same every step)
+        if (gwarp < P64 / 4 && (tid >> 5) < XH) xfill(a.eHA, a.eHB, fc, gwarp * 4 + cq, t);
     }
     __syncthreads();
 
-    // lane block at step t: lane f is in A for t < LA, lane c in B for t < LB
-    auto sh_f = [&](int st) { return st < a.LA ? ehA : ehB; };          // the rows' tables (shared)
-    auto sh_c = [&](int st) { return st < a.LB ? ehB : ehA; };
+    // block (0 A, 1 B, 2 C) of a lane at step st: lane f runs A then B, switching
+    // at LA, and lane c B then A, switching at LB; for a linear ABC triblock
+    // lane f runs A, B, C switching at LA and LA + LB, and lane c C, B, A
+    // switching at LC and LC + LB
+    auto blk_f = [&](int st) { return st < a.LA ? 0 : (!TRI || st < a.LA + a.LB) ? 1 : 2; };
+    auto blk_c = [&](int st) { return TRI ? (st < a.LC ? 2 : st < a.LC + a.LB ? 1 : 0) : (st < a.LB ? 1 : 0); };
+    auto gl_of = [&](int k) { return k == 0 ? a.eHA : k == 1 ? a.eHB : a.eHC; };
+    // the rows' tables (shared) of lane f's and lane c's block
+    auto sh_f = [&](int st) {
+        if constexpr (TRI) {
+            const int k = blk_f(st);
+            return k == 0 ? ehA : k == 1 ? ehB : ehC;
+        } else {
+            return st < a.LA ? ehA : ehB;
+        }
+    };
+    auto sh_c = [&](int st) {
+        if constexpr (TRI) {
+            const int k = blk_c(st);
+            return k == 0 ? ehA : k == 1 ? ehB : ehC;
+        } else {
+            return st < a.LB ? ehB : ehA;
+        }
+    };
 
     auto gsync = [&]() { grid_sync(ctr, a.err, ++bidx, stopped); };
 
@@ -418,9 +454,16 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
                     atomicExch(a.err, 4);
                     break;
                 }
-                if (task < P64 / 4)
-                    xtask_half(a.Z2, a.Z3, st >= a.LA, st < a.LB, scratch, fc, task * 4 + cq, t, tw, tab, rMd);
-                else
+                if (task < P64 / 4) {
+                    if constexpr (TRI) {
+                        // the warp's factor pairs, again whenever a lane changes block
+                        if (st == 0 || blk_f(st) != blk_f(st - 1) || blk_c(st) != blk_c(st - 1))
+                            xfill(gl_of(blk_f(st)), gl_of(blk_c(st)), fc, task * 4 + cq, t);
+                        xtask_half(a.Z2, a.Z3, false, true, scratch, fc, task * 4 + cq, t, tw, tab, rMd);
+                    } else {
+                        xtask_half(a.Z2, a.Z3, st >= a.LA, st < a.LB, scratch, fc, task * 4 + cq, t, tw, tab, rMd);
+                    }
+                } else
                     xtask_full(a.Z1, scratch, (task - P64 / 4) * 4 + cq, t, tw, tab);
             }
             gsync();
@@ -507,11 +550,11 @@ __global__ void __launch_bounds__(NT, 1) sweep64_kernel(SweepArgs a, const doubl
 // sweep with an error instead of spinning on.  (The cooperative launch
 // attribute is not combined with the cluster dimension: profilers refuse such
 // launches.)
-cudaLaunchConfig_t sweep64_config(int grid, cudaStream_t st, cudaLaunchAttribute* attr) {
+cudaLaunchConfig_t sweep64_config(int grid, int smem, cudaStream_t st, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid, 1, 1);
     cfg.blockDim = dim3(NT, 1, 1);
-    cfg.dynamicSmemBytes = SMEM64;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 2;
@@ -526,15 +569,31 @@ cudaLaunchConfig_t sweep64_config(int grid, cudaStream_t st, cudaLaunchAttribute
 
 bool sweep64_supported(int Lx, int Ly, int Lz) { return Lx == 64 && Ly == 64 && Lz == 64; }
 
+std::vector<double> sweep64_axis_tables(const double l[3], double ds) {
+    const double PI = 3.14159265358979323846;
+    std::vector<double> tab(6 * 64);
+    for (int half = 0; half < 2; half++)
+        for (int ax = 0; ax < 3; ax++) {
+            const double cc = -4.0 * PI * PI / (l[ax] * l[ax]);
+            const double h = half ? 0.5 * ds : ds;
+            for (int i = 0; i < 64; i++) {
+                const int ri = (i < 64 / 2 + 1) ? i : 64 - i;
+                tab[half * 192 + ax * 64 + i] = exp(h * (cc * ri * ri));
+            }
+        }
+    return tab;
+}
+
 int sweep64_prepare() {
-    PS_CUDA(cudaFuncSetAttribute(sweep64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM64));
+    PS_CUDA(cudaFuncSetAttribute(sweep64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM64));
+    PS_CUDA(cudaFuncSetAttribute(sweep64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM64_ABC));
     int dev = 0, sms = 0;
     PS_CUDA(cudaGetDevice(&dev));
     PS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = sweep64_config(sms & ~1, nullptr, attr);
+    cudaLaunchConfig_t cfg = sweep64_config(sms & ~1, SMEM64_ABC, nullptr, attr);
     int nclusters = 0;
-    PS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, sweep64_kernel, &cfg));
+    PS_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, sweep64_kernel<true>, &cfg));
     nclusters = std::min(nclusters, sms / 2);
     // 64 clusters own the slabs; every x-pass warp with a half-step task keeps
     // its factors resident, so the 2048 tasks need one warp each among the
@@ -552,8 +611,11 @@ void sweep64_launch(const SweepArgs& a0, const double* tables, int grid, cudaStr
     SweepArgs a = a0;
     a.twx = a.twy = a.twz = twiddle_table(64);
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = sweep64_config(grid, st, attr);
-    PS_CUDA(cudaLaunchKernelEx(&cfg, sweep64_kernel, a, tables));
+    cudaLaunchConfig_t cfg = sweep64_config(grid, a.eHC ? SMEM64_ABC : SMEM64, st, attr);
+    if (a.eHC)
+        PS_CUDA(cudaLaunchKernelEx(&cfg, sweep64_kernel<true>, a, tables));
+    else
+        PS_CUDA(cudaLaunchKernelEx(&cfg, sweep64_kernel<false>, a, tables));
 }
 
 }  // namespace ps

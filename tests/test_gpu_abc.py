@@ -40,9 +40,12 @@ def test_uniform_fields_are_exact(ps):
         assert np.abs(m.get(name) - fx).max() < 5e-14
 
 
+# the 64^3 case runs on the 64^3 sweep (three factor sets), the 32^3 one on
+# the generic sweep, the others on line passes
 CASES = [(2, (32, 32, 1), (4.0, 4.0), (21, 31, 11), "EM"), (2, (24, 48, 1), (3.6, 4.4), (20, 24, 17), "Anderson"),
          (3, (16, 24, 32), (3.5, 3.8, 4.1), (21, 22, 23), "Anderson"), (3, (32, 32, 32), (4.2, 4.2, 4.2),
-                                                                          (41, 45, 43), "Anderson")]
+                                                                          (41, 45, 43), "Anderson"),
+         (3, (64, 64, 64), (4.2, 4.4, 4.6), (21, 16, 25), "Anderson")]
 
 
 @pytest.mark.parametrize("dim,shape,L,Ms,scft", CASES)
@@ -93,8 +96,9 @@ def test_c_block_of_b_chemistry_is_the_device_ab_diblock(ps):
 
 def test_mixed_batch_members_equal_their_single_solves(ps):
     """AB and ABC solves in one batch (ps_batch_ab_create_mixed): the ABC
-    members run in grouped line-pass launches and equal their single solves
-    bit for bit; the AB members likewise."""
+    members run in shared generic-sweep launches (32^3, 48^3), their own
+    64^3 sweep (64^3) or grouped line-pass launches (64^2), and equal their
+    single solves bit for bit; the AB members likewise."""
     rng = np.random.default_rng(9)
     ab = [dict(dim=3, shape=(32, 32, 32), cell=ps.make_cell(3, "CUBIC", 4.0), Ms=(21, 45), chiN=16.0,
                scft="Anderson", n_anderson=10),
@@ -105,7 +109,9 @@ def test_mixed_batch_members_equal_their_single_solves(ps):
            dict(dim=3, shape=(48, 48, 48), cell=ps.make_cell(3, "CUBIC", 4.8), Ms=(33, 30, 31),
                 chi=(15.0, 20.0, 12.0), scft="Anderson", n_anderson=10),
            dict(dim=2, shape=(64, 64, 1), cell=ps.make_cell(2, "SQUARE", 4.0), Ms=(21, 21, 21),
-                chi=(20.0, 20.0, 20.0), scft="EM")]
+                chi=(20.0, 20.0, 20.0), scft="EM"),
+           dict(dim=3, shape=(64, 64, 64), cell=ps.make_cell(3, "CUBIC", 4.6), Ms=(17, 26, 21),
+                chi=(16.0, 19.0, 22.0), scft="Anderson", n_anderson=10)]
     b = ps.BatchAB(ab, abc)
     fields = []
     for k, sv in enumerate(ab + abc):
@@ -132,10 +138,12 @@ def test_mixed_batch_members_equal_their_single_solves(ps):
         assert b.residual_error(k) == m.residual_error()
 
 
-def test_sweep_and_line_passes_agree(ps, monkeypatch):
-    """A 32^3 triblock on the generic persistent sweep (three factor sets a
-    lane) and on the packed line passes (PS_B200_LINE_PASSES=1 at creation)."""
-    shape = (32, 32, 32)
+@pytest.mark.parametrize("n", [32, 64])
+def test_sweep_and_line_passes_agree(ps, monkeypatch, n):
+    """A 32^3 triblock on the generic persistent sweep and a 64^3 one on the
+    64^3 sweep (three factor sets a lane), against the packed line passes
+    (PS_B200_LINE_PASSES=1 at creation)."""
+    shape = (n, n, n)
     w = 0.1 * np.random.default_rng(4).standard_normal((3,) + shape)
     args = dict(dim=3, shape=shape, cell=ps.make_cell(3, "CUBIC", 4.2), Ms=(31, 25, 29), chi=(16.0, 22.0, 13.0),
                 scft="Anderson", n_anderson=10)
