@@ -13,7 +13,7 @@ spline re-sampling step over the whole string itself (polystring_AB.cc:
 strings, equal to the single-rank run.
 
 The exchange goes through torch.distributed (NCCL on GPUs, device tensors; gloo
-on the CPU for the tests).  No peer-memory loads and no multicast are used.
+on the CPU for the tests); the kernels read only their own GPU's memory.
 
 A backend supplies the per-rank work:
 
