@@ -244,10 +244,12 @@ def cpu_batch_baseline(seconds, threads, n=256):
                       % (threads, ", ".join(samples))}
 
 
-def string_method(ps, fp64=(37.0, "nominal"), iters=10):
+def string_method(ps, fp64=(37.0, "nominal"), iters=200, seq_reps=3):
     """Secondary result: the batched string method (40 images, 2D 128x128,
-    Ns 128, 3 SCFT iterations per image per string iteration) against the
-    same SCFT work run image by image through the plain single-model path."""
+    Ns 128, 3 SCFT iterations per image per string iteration; the config's
+    200 string iterations timed) against the same SCFT work run image by image
+    through the plain single-model path (seq_reps string iterations' worth,
+    averaged)."""
     from polystring_b200 import workloads
     m, shape, L = 40, (128, 128, 1), 8.0
     Ms = workloads.ms_from(0.35, 128)
@@ -266,11 +268,12 @@ def string_method(ps, fp64=(37.0, "nominal"), iters=10):
     single.update(3)
     single.synchronize()
     t0 = time.perf_counter()
-    for s in range(m):
-        single.set_fields(wa[s], wb[s])
-        single.update(3)
-        single.H()
-    ts = time.perf_counter() - t0
+    for rep in range(seq_reps):
+        for s in range(m):
+            single.set_fields(wa[s], wb[s])
+            single.update(3)
+            single.H()
+    ts = (time.perf_counter() - t0) / seq_reps
     # the whole string iteration as propagator work: 2 Ns steps of M points
     # per image and SCFT iteration, 15 log2(M) + 20 FP64 flops each
     import math
@@ -285,6 +288,7 @@ def string_method(ps, fp64=(37.0, "nominal"), iters=10):
                      "note": "whole string iteration (densities, mixing, spline included) counted as propagation"},
             "speedup_vs_sequential": ts / tb, "launches_per_string_iteration": g.launches_per_iteration(),
             "propagator_path": [l for l in ps.lib().ps_tuning_log().decode().split("\ngrid ") if "128x128x1" in l],
+            "string_iterations_timed": iters, "sequential_string_iterations_timed": seq_reps,
             "timing": "host wall clock around synchronised replays"}
 
 
